@@ -1,0 +1,727 @@
+// Host side of the engine: resident tables, parameter conversion, workspace,
+// and the plain / batched profile paths behind the C ABI of include/ppm.h.
+//
+// Replaces the reference's table constructors (gpu/lensing.cuh:27-54,
+// gpu/nsx.cuh:83-128, gpu/ism_inst.cuh:18-32) and calc_one_star
+// (gpu/devarshi24st_gpu.cu:432-511, gpu/os1_gpu.cu:304-349).  All device
+// memory is owned by the engine; every error becomes a status code.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ppm.h"
+#include "common.h"
+#include "engine.h"
+#include "kernels.cuh"
+
+namespace ppm {
+
+using namespace units;
+
+#define PPM_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      throw Error(PPM_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));              \
+  } while (0)
+
+template <class T>
+static T* dev_alloc(size_t n) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  if (e != cudaSuccess) throw Error(PPM_E_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return (T*)p;
+}
+
+template <class T>
+static T* dev_upload(const T* h, size_t n) {
+  T* d = dev_alloc<T>(n);
+  cudaError_t e = cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) throw Error(PPM_E_CUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+  return d;
+}
+
+void DeviceBuffer::reserve(size_t bytes) {
+  if (bytes <= cap) return;
+  size_t want = std::max(bytes, cap + cap / 2);
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  cap = 0;
+  cudaError_t e = cudaMalloc(&ptr, want);
+  if (e != cudaSuccess) throw Error(PPM_E_OOM, std::string("cudaMalloc workspace: ") + cudaGetErrorString(e));
+  cap = want;
+}
+void DeviceBuffer::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  cap = 0;
+}
+void HostBuffer::reserve(size_t bytes) {
+  if (bytes <= cap) return;
+  if (ptr) cudaFreeHost(ptr);
+  ptr = nullptr;
+  cap = 0;
+  cudaError_t e = cudaMallocHost(&ptr, bytes);
+  if (e != cudaSuccess) throw Error(PPM_E_OOM, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+  cap = bytes;
+}
+void HostBuffer::release() {
+  if (ptr) cudaFreeHost(ptr);
+  ptr = nullptr;
+  cap = 0;
+}
+
+Engine::Engine(const ppm_engine_config& c) : cfg(c) {
+  if (cfg.memory_budget <= 0) cfg.memory_budget = 64ll << 30;
+  if (cfg.n_streams <= 0) cfg.n_streams = 4;
+  if (cfg.max_batch <= 0) cfg.max_batch = 1 << 16;
+  int n_dev = 0;
+  PPM_CUDA(cudaGetDeviceCount(&n_dev));
+  if (cfg.device < 0 || cfg.device >= n_dev) throw Error(PPM_E_INVALID, "no such CUDA device");
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  PPM_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, cfg.device));
+  PPM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  for (int k = 0; k < 3; ++k) PPM_CUDA(cudaEventCreate(&ev[k]));
+}
+
+Engine::~Engine() {
+  cudaSetDevice(cfg.device);
+  serve_shutdown();
+  cudaStreamSynchronize(stream);
+  for (void* p : owned) cudaFree(p);
+  for (auto& kv : ring_tabs) cudaFree(kv.second);
+  for (auto& kv : fine_tabs) cudaFree(kv.second);
+  ws_prof.release();
+  ws_flux.release();
+  ws_counts.release();
+  ws_stats.release();
+  ws_tiles.release();
+  ws_ctrl.release();
+  ws_jobs.release();
+  h_stage.release();
+  h_out.release();
+  for (auto& g : graphs) cudaGraphExecDestroy(g.second.exec);
+  for (int k = 0; k < 3; ++k) cudaEventDestroy(ev[k]);
+  cudaStreamDestroy(stream);
+}
+
+void Engine::track(void* p) { owned.push_back(p); }
+
+// ---- tables ------------------------------------------------------------------
+void Engine::load_lensing(const ppm_lensing_desc& d) {
+  if (d.n_u < 2 || d.n_cos_psi < 2 || d.n_cos_alpha < 2 || !d.cos_alpha_of_u_cos_psi || !d.lf_of_u_cos_psi ||
+      !d.cdt_over_R_of_u_cos_alpha)
+    throw Error(PPM_E_INVALID, "lensing table: need >= 2 points per axis and all three matrices");
+  if (!(d.u_min < d.u_max && d.cos_psi_min < d.cos_psi_max && d.cos_alpha_min < d.cos_alpha_max))
+    throw Error(PPM_E_INVALID, "lensing table: axis min must be below max");
+  if (d.n_cos_psi > 4096 || d.n_cos_alpha > 4096) throw Error(PPM_E_RANGE, "lensing table: at most 4096 points per angle axis");
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  PPM_CUDA(cudaStreamSynchronize(stream));
+  DevLens L{};
+  L.u_min = d.u_min;
+  L.u_max = d.u_max;
+  L.cp_min = d.cos_psi_min;
+  L.cp_max = d.cos_psi_max;
+  L.ca_min = d.cos_alpha_min;
+  L.ca_max = d.cos_alpha_max;
+  L.n_u = d.n_u;
+  L.n_cp = d.n_cos_psi;
+  L.n_ca = d.n_cos_alpha;
+  double* ca = dev_upload(d.cos_alpha_of_u_cos_psi, (size_t)d.n_u * d.n_cos_psi);
+  double* lf = dev_upload(d.lf_of_u_cos_psi, (size_t)d.n_u * d.n_cos_psi);
+  double* cdt = dev_upload(d.cdt_over_R_of_u_cos_alpha, (size_t)d.n_u * d.n_cos_alpha);
+  track(ca);
+  track(lf);
+  track(cdt);
+  L.ca = ca;
+  L.lf = lf;
+  L.cdt = cdt;
+  lens = L;
+  has_lens = true;
+}
+
+void Engine::load_nsx(const ppm_nsx_desc& d) {
+  if (d.n_logT < 2 || d.n_logg < 2 || d.n_logEkT < 4 || d.n_mu < 4 || !d.mu || !d.log_I_T3)
+    throw Error(PPM_E_INVALID, "NSX table: need >= 2 logT/logg points, >= 4 logEkT/mu points and data");
+  for (int i = 0; i + 1 < d.n_mu; ++i)
+    if (!(d.mu[i] > d.mu[i + 1])) throw Error(PPM_E_INVALID, "NSX table: mu must be strictly descending (cpu/nsx.hpp:142-147)");
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  PPM_CUDA(cudaStreamSynchronize(stream));
+  const size_t slice = (size_t)d.n_logEkT * d.n_mu;
+  const size_t stride = (slice + 3) / 4 * 4;
+  const size_t n_sl = (size_t)d.n_logT * d.n_logg;
+  // values 10^logInuT3 (cpu/nsx.hpp:134) scaled by a power of two so the largest is O(1) in FP32
+  std::vector<double> lin(slice * n_sl);
+  double vmax = 0.0;
+  for (size_t k = 0; k < lin.size(); ++k) {
+    lin[k] = std::pow(10, d.log_I_T3[k]);
+    if (std::isfinite(lin[k])) vmax = std::max(vmax, std::fabs(lin[k]));
+  }
+  int e2 = 0;
+  if (vmax > 0) std::frexp(vmax, &e2);
+  const int scale_exp = -e2;
+  std::vector<float> h(stride * n_sl, 0.0f);
+  for (size_t sl = 0; sl < n_sl; ++sl)
+    for (size_t k = 0; k < slice; ++k) h[sl * stride + k] = (float)std::ldexp(lin[sl * slice + k], scale_exp);
+  float* data = dev_upload(h.data(), h.size());
+  double* mu = dev_upload(d.mu, (size_t)d.n_mu);
+  track(data);
+  track(mu);
+  DevNsx X{};
+  X.nT = d.n_logT;
+  X.ng = d.n_logg;
+  X.nE = d.n_logEkT;
+  X.nmu = d.n_mu;
+  X.slice_stride = (int)stride;
+  X.T_min = d.logT_min;
+  X.T_max = d.logT_max;
+  X.g_min = d.logg_min;
+  X.g_max = d.logg_max;
+  X.E_min = d.logEkT_min;
+  X.E_max = d.logEkT_max;
+  X.inv_dE = (d.n_logEkT - 1) / (d.logEkT_max - d.logEkT_min);
+  X.data = data;
+  X.mu = mu;
+  X.scale_exp = scale_exp;
+  nsx = X;
+  nsx_mu.assign(d.mu, d.mu + d.n_mu);
+  has_nsx = true;
+  ++nsx_version;
+}
+
+int Engine::add_grid(int n_e, const double* E) {
+  if (n_e < 1 || !E) throw Error(PPM_E_INVALID, "energy grid: need at least one energy");
+  if (n_e > 2048) throw Error(PPM_E_RANGE, "energy grid: at most 2048 energies");
+  for (int i = 0; i < n_e; ++i)
+    if (!(E[i] > 0) || !std::isfinite(E[i])) throw Error(PPM_E_INVALID, "energy grid: energies must be positive");
+  Grid g;
+  g.E.assign(E, E + n_e);
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  g.dE = dev_upload(E, n_e);
+  std::vector<double> inv(n_e);
+  for (int i = 0; i < n_e; ++i) inv[i] = 1.0 / E[i];
+  g.dinvE = dev_upload(inv.data(), n_e);
+  track(g.dE);
+  track(g.dinvE);
+  grids.push_back(std::move(g));
+  return (int)grids.size() - 1;
+}
+
+// Per-energy split of t_E = log10(E) (n_E - 1)/(logEkT_max - logEkT_min) for the loaded NSX axis.
+void Engine::prepare_grid(int id) {
+  Grid& g = grids[id];
+  if (!has_nsx) return;
+  if (g.nsx_version == nsx_version) return;
+  const int n = (int)g.E.size();
+  std::vector<int> iE(n), rE(n);
+  std::vector<float> fE(n);
+  double lo = 1e300, hi = -1e300;
+  int imin = 1 << 30, imax = -(1 << 30);
+  for (int i = 0; i < n; ++i) {
+    double t = std::log10(g.E[i]) * nsx.inv_dE;
+    double fl = std::floor(t);
+    iE[i] = (int)fl;
+    fE[i] = (float)(t - fl);
+    if (fE[i] >= 1.0f) {  // rounding of the fraction up to 1
+      fE[i] = 0.0f;
+      iE[i] += 1;
+    }
+    lo = std::min(lo, t);
+    hi = std::max(hi, t);
+    imin = std::min(imin, iE[i]);
+    imax = std::max(imax, iE[i]);
+  }
+  for (int i = 0; i < n; ++i) rE[i] = iE[i] - imin;
+  if (g.drE) cudaFree(g.drE);
+  if (g.dfE) cudaFree(g.dfE);
+  g.drE = dev_upload(rE.data(), n);
+  g.dfE = dev_upload(fE.data(), n);
+  g.iE_min = imin;
+  g.span = imax - imin + 1;
+  g.tE_lo = lo;
+  g.tE_hi = hi;
+  g.nsx_version = nsx_version;
+}
+
+DevGrid Engine::dev_grid(int id) {
+  Grid& g = grids[id];
+  DevGrid d{};
+  d.n_e = (int)g.E.size();
+  d.iE_min = g.iE_min;
+  d.span = g.span;
+  d.tE_lo = g.tE_lo;
+  d.tE_hi = g.tE_hi;
+  d.E = g.dE;
+  d.invE = g.dinvE;
+  d.rE = g.drE;
+  d.fE = g.dfE;
+  return d;
+}
+
+int Engine::add_response(int grid, int n_ch, const double* rsp) {
+  if (grid < 0 || grid >= (int)grids.size()) throw Error(PPM_E_INVALID, "response: unknown energy grid");
+  if (n_ch < 1 || !rsp) throw Error(PPM_E_INVALID, "response: need channels and a matrix");
+  if (n_ch > 8192) throw Error(PPM_E_RANGE, "response: at most 8192 channels");
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  Resp r;
+  r.grid = grid;
+  r.n_ch = n_ch;
+  r.n_e = (int)grids[grid].E.size();
+  r.d_rsp = dev_upload(rsp, (size_t)n_ch * r.n_e);
+  track(r.d_rsp);
+  r.h_rsp.assign(rsp, rsp + (size_t)n_ch * r.n_e);
+  fold_tc_prepare(r);
+  resps.push_back(std::move(r));
+  return (int)resps.size() - 1;
+}
+
+// (z, cos(acos z), sin(acos z)) of every ring, computed with the host libm as
+// the reference's GenerateHealpixGrid does (cpu/grid.hpp:219-244,254).
+const double* Engine::ring_table(int N) {
+  auto it = ring_tabs.find(N);
+  if (it != ring_tabs.end()) return it->second;
+  std::vector<double> h(3 * (size_t)4 * N, 0.0);
+  for (int i = 1; i <= 4 * N - 1; ++i) {
+    int ii = i > 2 * N ? 4 * N - i : i;
+    double z = ii < N ? 1. - 1. * ii * ii / (3. * N * N) : 4. / 3. - 2. * ii / (3. * N);
+    if (i > 2 * N) z = -z;
+    double th = std::acos(z);
+    h[3 * i] = z;
+    h[3 * i + 1] = std::cos(th);
+    h[3 * i + 2] = std::sin(th);
+  }
+  host_rings[N] = h;
+  double* d = dev_upload(h.data(), h.size());
+  ring_tabs[N] = d;
+  return d;
+}
+
+// (cos, sin) of 2 pi k / n_fine (cpu/devarshi24st_cpu.cpp:131-134).
+const double* Engine::fine_table(int nf) {
+  auto it = fine_tabs.find(nf);
+  if (it != fine_tabs.end()) return it->second;
+  std::vector<double> h(2 * (size_t)nf);
+  for (int k = 0; k < nf; ++k) {
+    double phase = 1. * k / nf;
+    double spot_phi = two_pi * phase;
+    h[2 * k] = std::cos(spot_phi);
+    h[2 * k + 1] = std::sin(spot_phi);
+  }
+  double* d = dev_upload(h.data(), h.size());
+  fine_tabs[nf] = d;
+  return d;
+}
+
+// ---- parameters -----------------------------------------------------------------
+void Engine::validate(const ppm_params& p) const {
+  if (!has_lens) throw Error(PPM_E_STATE, "lensing tables not loaded");
+  if (p.n_spots < 1 || p.n_spots > 2) throw Error(PPM_E_INVALID, "n_spots must be 1 or 2");
+  if (p.atmosphere != PPM_ATM_NSX && p.atmosphere != PPM_ATM_BLACKBODY) throw Error(PPM_E_INVALID, "unknown atmosphere");
+  if (p.atmosphere == PPM_ATM_NSX && !has_nsx) throw Error(PPM_E_STATE, "NSX table not loaded");
+  if (p.atmosphere == PPM_ATM_NSX && p.precision != PPM_PREC_FP32)
+    throw Error(PPM_E_INVALID, "the NSX integrand runs in FP32 (precision must be PPM_PREC_FP32)");
+  if (p.interp < 0 || p.interp > 4) throw Error(PPM_E_INVALID, "unknown NSX interpolator");
+  if (p.atmosphere == PPM_ATM_NSX && (p.interp <= 2) && (nsx.nT < 4 || nsx.ng < 4))
+    throw Error(PPM_E_RANGE, "cubic logT/logg interpolation needs >= 4 points on both axes");
+  if (p.beaming < 0 || p.beaming > 2) throw Error(PPM_E_INVALID, "unknown beaming");
+  if (p.precision != PPM_PREC_FP32 && p.precision != PPM_PREC_FP64) throw Error(PPM_E_INVALID, "unknown precision");
+  if (p.fold < 0 || p.fold > 2) throw Error(PPM_E_INVALID, "unknown fold");
+  if (p.n_side < 1 || p.n_side > 8192) throw Error(PPM_E_RANGE, "n_side must be in [1, 8192]");
+  if (p.n_bins < 1 || p.n_bins > 4096) throw Error(PPM_E_RANGE, "n_bins must be in [1, 4096]");
+  if (p.n_gl < 0 || p.n_gl > 6) throw Error(PPM_E_RANGE, "n_gl must be in [0, 6] (cpu/gl.hpp)");
+  if (p.n_fine < 2 || p.n_fine > 4096) throw Error(PPM_E_RANGE, "n_fine must be in [2, 4096]");
+  if (p.energy_grid < 0 || p.energy_grid >= (int)grids.size()) throw Error(PPM_E_INVALID, "unknown energy grid");
+  if (p.response >= (int)resps.size() || p.response < -1) throw Error(PPM_E_INVALID, "unknown response");
+  if (p.response >= 0 && resps[p.response].grid != p.energy_grid)
+    throw Error(PPM_E_INVALID, "response is defined on another energy grid");
+  if (!(p.mass_msun > 0) || !(p.r_eq_km > 0) || !(p.spin_hz >= 0) || !(p.distance_kpc > 0))
+    throw Error(PPM_E_INVALID, "mass, radius and distance must be positive");
+  if (!(p.mass_msun * schwarzschild_radius_of_sun_in_km < p.r_eq_km))
+    throw Error(PPM_E_RANGE, "star inside its Schwarzschild radius");
+  for (int s = 0; s < p.n_spots; ++s) {
+    const ppm_spot& sp = p.spots[s];
+    if (sp.kind != PPM_SPOT_HEALPIX && sp.kind != PPM_SPOT_POINT) throw Error(PPM_E_INVALID, "unknown spot kind");
+    if (p.atmosphere == PPM_ATM_BLACKBODY && !(sp.kT_keV > 0)) throw Error(PPM_E_INVALID, "blackbody spot needs kT_keV > 0");
+    if (!std::isfinite(sp.theta1) || !std::isfinite(sp.angrad1) || !std::isfinite(sp.logT))
+      throw Error(PPM_E_INVALID, "non-finite spot parameter");
+  }
+}
+
+void Engine::to_device(const ppm_params& p, DevProfile& d, long long flux_off, unsigned long long* stats) {
+  std::memset(&d, 0, sizeof(d));
+  // cpu/devarshi24st_cpu.cpp:48-74
+  const double M = p.mass_msun, Re = p.r_eq_km, frequency_nu = p.spin_hz;
+  const double D = p.distance_kpc * kpc_in_km;
+  double Rs = M * schwarzschild_radius_of_sun_in_km;
+  double ue = Rs / Re;
+  double uue = std::sqrt(1. - ue);
+  double logg0 = std::log10(M / (Re * Re * uue));
+  double logGMsun_s2_km2cm = std::log10(1.32712440041279419E16);
+  double Omega_bar = two_pi * frequency_nu * std::sqrt(Re * Re * Re / M) * sqrt_km3_over_s2_GMsun;
+  double x = 0.5 * Rs / Re;
+  double o2 = Omega_bar * Omega_bar * (-0.788 + 1.030 * x);
+  d.Re = Re;
+  d.Rs = Rs;
+  d.nu = frequency_nu;
+  d.o2 = o2;
+  d.D2 = D * D;
+  d.cos_obs = std::cos(p.inclination_rad);
+  d.sin_obs = std::sin(p.inclination_rad);
+  d.dOmega_hp = pi / (3. * p.n_side * p.n_side);
+  const double c0e = -0.791, c1e = 0.776, c0p = 1.138, c1p = -1.431, d1e = -1.315, d2e = 2.431, f1e = -1.172,
+               d1p = 0.653, d2p = -2.864, f1p = 0.975, d160 = 13.47, d260 = -27.13;
+  d.ce = c0e + c1e * x;
+  d.cp = c0p + c1p * x;
+  d.de = d1e * x + d2e * x * x;
+  d.fe = f1e * x;
+  d.dp = d1p * x + d2p * x * x;
+  d.fp = f1p * x;
+  d.d60 = d160 * x + d260 * x * x;
+  d.Ob2 = Omega_bar * Omega_bar;
+  d.Ob4 = d.Ob2 * d.Ob2;
+  d.Ob6 = d.Ob4 * d.Ob2;
+  d.logg_base = logg0 + logGMsun_s2_km2cm;
+  d.n_side = p.n_side;
+  d.n_bins = p.n_bins;
+  d.n_gl = p.n_gl;
+  d.n_fine = p.n_fine;
+  d.n_spots = p.n_spots;
+  d.atmosphere = p.atmosphere;
+  d.interp = p.interp;
+  d.beaming = p.beaming;
+  d.precision = p.precision;
+  d.flux_off = flux_off;
+  d.ring = ring_table(p.n_side);
+  d.fine = fine_table(p.n_fine);
+  prepare_grid(p.energy_grid);
+  d.grid = dev_grid(p.energy_grid);
+  d.n_e = d.grid.n_e;
+  d.stats = stats;
+  const bool nsx_atm = p.atmosphere == PPM_ATM_NSX;
+  const std::vector<double>& rt = host_rings[p.n_side];
+  for (int s = 0; s < p.n_spots; ++s) {
+    const ppm_spot& sp = p.spots[s];
+    DevSpot& o = d.spot[s];
+    o.kind = sp.kind;
+    // IsInside (cpu/grid.hpp:158-167) evaluates these with the host libm
+    o.s1 = std::sin(sp.theta1);
+    o.c1 = std::cos(sp.theta1);
+    o.ph1 = sp.phi1;
+    o.cos_ar1 = std::cos(sp.angrad1);
+    o.s2 = std::sin(sp.theta2);
+    o.c2 = std::cos(sp.theta2);
+    o.ph2 = sp.phi2;
+    o.cos_ar2 = std::cos(sp.angrad2);
+    double sin_half_ar = std::sin(0.5 * sp.angrad1);
+    o.cos_theta_pt = std::cos(sp.theta1);
+    o.dOmega_pt = two_pi * 2. * sin_half_ar * sin_half_ar;  // cpu/grid.hpp:19-22
+    double logT = sp.logT;
+    o.kT = nsx_atm ? std::pow(10, logT) * 8.617333262E-8 : sp.kT_keV;
+    o.l10kT = std::log10(o.kT);
+    if (nsx_atm)
+      o.out_scale = (1.0 / d.D2) * (std::pow(10, 3 * logT) / planck) * std::ldexp(1.0, -nsx.scale_exp);
+    else
+      o.out_scale = Ibb_constant / d.D2;
+    // ring range that can hold elements of disk 1
+    if (sp.kind == PPM_SPOT_HEALPIX) {
+      // disk 1 lies within |theta - theta1| <= angrad1; one ring of margin on each side
+      const int N = p.n_side, nr = 4 * N - 1;
+      const double t1 = sp.theta1, r1 = std::fabs(sp.angrad1);
+      const bool all = !(t1 >= 0 && t1 <= pi) || r1 >= pi;
+      const double zhi = (all || t1 - r1 <= 0) ? 2.0 : std::cos(t1 - r1) + 1e-9;
+      const double zlo = (all || t1 + r1 >= pi) ? -2.0 : std::cos(t1 + r1) - 1e-9;
+      int ilo = nr + 1, ihi = 0;
+      for (int i = 1; i <= nr; ++i) {
+        const double z = rt[3 * i];
+        if (z <= zhi && z >= zlo) {
+          ilo = std::min(ilo, i);
+          ihi = std::max(ihi, i);
+        }
+      }
+      if (ilo > ihi) {
+        o.i_lo = 1;
+        o.i_hi = 0;
+      } else {
+        o.i_lo = std::max(1, ilo - 1);
+        o.i_hi = std::min(nr, ihi + 1);
+      }
+    }
+    if (nsx_atm) {
+      // logT taps (cpu/nsx.hpp:174-187 cubic, 250-285 linear)
+      double xT = logT, aT;
+      int iT;
+      o.T_clamped = (xT < nsx.T_min || xT > nsx.T_max) ? 1 : 0;
+      if (xT <= nsx.T_min) {
+        aT = 0;
+        xT = nsx.T_min;
+        iT = 0;
+      } else if (xT >= nsx.T_max) {
+        aT = 1;
+        xT = nsx.T_max;
+        iT = nsx.nT - 2;
+      } else {
+        double t = (xT - nsx.T_min) / (nsx.T_max - nsx.T_min) * (nsx.nT - 1);
+        iT = (int)t;
+        aT = t - iT;
+      }
+      const bool cubic = p.interp <= 2;
+      if (cubic) {
+        int i0 = std::min(std::max(iT - 1, 0), nsx.nT - 4);
+        auto node = [&](int i) { return nsx.T_min + (nsx.T_max - nsx.T_min) * i / (nsx.nT - 1); };
+        double x0 = node(i0), x1 = node(i0 + 1), x2 = node(i0 + 2), x3 = node(i0 + 3);
+        o.wT[0] = (xT - x1) * (xT - x2) * (xT - x3) / ((x0 - x1) * (x0 - x2) * (x0 - x3));
+        o.wT[1] = (xT - x0) * (xT - x2) * (xT - x3) / ((x1 - x0) * (x1 - x2) * (x1 - x3));
+        o.wT[2] = (xT - x0) * (xT - x1) * (xT - x3) / ((x2 - x0) * (x2 - x1) * (x2 - x3));
+        o.wT[3] = (xT - x0) * (xT - x1) * (xT - x2) / ((x3 - x0) * (x3 - x1) * (x3 - x2));
+        for (int k = 0; k < 4; ++k) o.iT[k] = i0 + k;
+        o.nT_taps = 4;
+      } else {
+        o.iT[0] = iT;
+        o.iT[1] = iT + 1;
+        o.wT[0] = 1 - aT;
+        o.wT[1] = aT;
+        o.nT_taps = 2;
+      }
+    }
+  }
+}
+
+// ---- workspace and launches ----------------------------------------------------------
+long long Engine::tile_bound(const ppm_params& p, int chunk) {
+  long long b = 0;
+  const int N = p.n_side;
+  const std::vector<double>& rt = host_rings[N];
+  (void)rt;
+  for (int s = 0; s < p.n_spots; ++s) {
+    if (p.spots[s].kind == PPM_SPOT_POINT) {
+      b += 1;
+      continue;
+    }
+    // rings in range x (two ranges + chunks per range)
+    long long rings = 4ll * N - 1;
+    long long per = 2 + (4ll * N + chunk - 1) / chunk;
+    b += rings * per;
+  }
+  return b;
+}
+
+void Engine::run(int n, const ppm_params* ps, double* ext_flux, double* ext_counts, Batch& B, cudaStream_t st) {
+  B.n = n;
+  B.flux_off.assign(n + 1, 0);
+  B.counts_off.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    validate(ps[i]);
+    ring_table(ps[i].n_side);
+    const long long ne = (long long)grids[ps[i].energy_grid].E.size();
+    B.flux_off[i + 1] = B.flux_off[i] + (long long)ps[i].n_bins * ne;
+    const long long nc = ps[i].response >= 0 ? (long long)resps[ps[i].response].n_ch * ps[i].n_bins : 0;
+    B.counts_off[i + 1] = B.counts_off[i] + nc;
+  }
+  // groups by kernel variant: 0 = NSX, 1 = blackbody FP64, 2 = blackbody FP32
+  std::vector<int> order;
+  order.reserve(n);
+  for (int v = 0; v < 3; ++v)
+    for (int i = 0; i < n; ++i) {
+      int var = ps[i].atmosphere == PPM_ATM_NSX ? 0 : (ps[i].precision == PPM_PREC_FP64 ? 1 : 2);
+      if (var == v) order.push_back(i);
+    }
+  const int chunk = tune.chunk;
+  // device profiles in group order
+  std::vector<DevProfile> hp(n);
+  ws_stats.reserve(sizeof(unsigned long long) * kStats * (size_t)n);
+  unsigned long long* d_stats = (unsigned long long*)ws_stats.ptr;
+  long long tiles_total = 0;
+  std::vector<long long> tiles_group(3, 0);
+  std::vector<int> group_start(4, 0);
+  for (int k = 0; k < n; ++k) {
+    const int i = order[k];
+    to_device(ps[i], hp[k], B.flux_off[i], d_stats + (size_t)kStats * i);
+    int var = ps[i].atmosphere == PPM_ATM_NSX ? 0 : (ps[i].precision == PPM_PREC_FP64 ? 1 : 2);
+    tiles_group[var] += tile_bound(ps[i], chunk);
+    group_start[var + 1] = k + 1;
+  }
+  for (int v = 1; v <= 3; ++v) group_start[v] = std::max(group_start[v], group_start[v - 1]);
+  for (int v = 0; v < 3; ++v) tiles_total += tiles_group[v];
+  if (tiles_total > (1ll << 31) - 1) throw Error(PPM_E_RANGE, "batch too large for one work queue");
+
+  ws_prof.reserve(sizeof(DevProfile) * (size_t)n);
+  ws_flux.reserve(sizeof(double) * (size_t)std::max(1ll, B.flux_off[n]));
+  ws_counts.reserve(sizeof(double) * (size_t)std::max(1ll, B.counts_off[n]));
+  ws_tiles.reserve(sizeof(Tile) * (size_t)std::max(1ll, tiles_total));
+  ws_ctrl.reserve(sizeof(int) * 16);
+  // the pinned staging buffer may still feed the previous batch's copy
+  PPM_CUDA(cudaEventSynchronize(ev[0]));
+  h_stage.reserve(sizeof(DevProfile) * (size_t)n);
+  std::memcpy(h_stage.ptr, hp.data(), sizeof(DevProfile) * (size_t)n);
+  DevProfile* d_prof = (DevProfile*)ws_prof.ptr;
+  B.d_flux = ext_flux ? ext_flux : (double*)ws_flux.ptr;
+  B.d_counts = ext_counts ? ext_counts : (double*)ws_counts.ptr;
+  B.d_stats = d_stats;
+
+  PPM_CUDA(cudaMemcpyAsync(d_prof, h_stage.ptr, sizeof(DevProfile) * (size_t)n, cudaMemcpyHostToDevice, st));
+  PPM_CUDA(cudaEventRecord(ev[0], st));
+  PPM_CUDA(cudaMemsetAsync(B.d_flux, 0, sizeof(double) * (size_t)B.flux_off[n], st));
+  PPM_CUDA(cudaMemsetAsync(d_stats, 0, sizeof(unsigned long long) * kStats * (size_t)n, st));
+  PPM_CUDA(cudaMemsetAsync(ws_ctrl.ptr, 0, sizeof(int) * 16, st));
+  int* ctrl = (int*)ws_ctrl.ptr;
+
+  long long tile_base = 0;
+  for (int v = 0; v < 3; ++v) {
+    const int g0 = group_start[v], g1 = group_start[v + 1];
+    if (g1 <= g0) continue;
+    WorkQueue q{};
+    q.tiles = (Tile*)ws_tiles.ptr + tile_base;
+    q.capacity = (int)tiles_group[v];
+    q.n_tiles = ctrl + 3 * v;
+    q.next = ctrl + 3 * v + 1;
+    q.overflow = ctrl + 3 * v + 2;
+    tile_base += tiles_group[v];
+    PPM_CUDA(launch_plan(d_prof + g0, g1 - g0, lens, q, chunk, st));
+    // launch shape
+    int ne_max = 1, nf_max = 2, cells_max = 1;
+    for (int k = g0; k < g1; ++k) {
+      ne_max = std::max(ne_max, hp[k].n_e);
+      nf_max = std::max(nf_max, hp[k].n_fine);
+      cells_max = std::max(cells_max, hp[k].grid.span + 1);
+    }
+    KernelArgs a{};
+    a.profiles = d_prof + g0;
+    a.lens = lens;
+    a.nsx = nsx;
+    a.queue = q;
+    a.flux = B.d_flux;
+    a.shape = choose_shape(v == 0, v == 1, ne_max, nf_max, cells_max);
+    PPM_CUDA(configure_integrand_smem(a.shape));
+    int occ = max_active_ctas(a.shape);
+    if (occ < 1) throw Error(PPM_E_RANGE, "integrand launch shape does not fit on an SM (shared memory " +
+                                              std::to_string(a.shape.total) + " bytes)");
+    long long grid = std::min<long long>((long long)sm_count * occ, tiles_group[v]);
+    PPM_CUDA(launch_integrand(a, (int)grid, st));
+  }
+  // folds grouped by (response, n_bins, arithmetic)
+  std::map<std::tuple<int, int, int>, std::vector<FoldJob>> folds;
+  for (int i = 0; i < n; ++i) {
+    if (ps[i].response < 0) continue;
+    FoldJob j{B.flux_off[i], B.counts_off[i], ps[i].exposure_s * (1. / ps[i].n_bins)};
+    folds[std::make_tuple(ps[i].response, ps[i].n_bins, ps[i].fold)].push_back(j);
+  }
+  size_t njobs = 0;
+  for (auto& kv : folds) njobs += kv.second.size();
+  if (njobs) {
+    ws_jobs.reserve(sizeof(FoldJob) * njobs);
+    h_jobs.resize(njobs);
+    size_t k = 0;
+    for (auto& kv : folds)
+      for (auto& j : kv.second) h_jobs[k++] = j;
+    PPM_CUDA(cudaMemcpyAsync(ws_jobs.ptr, h_jobs.data(), sizeof(FoldJob) * njobs, cudaMemcpyHostToDevice, st));
+    k = 0;
+    for (auto& kv : folds) {
+      const Resp& r = resps[std::get<0>(kv.first)];
+      const int nb = std::get<1>(kv.first), mode = std::get<2>(kv.first);
+      const FoldJob* jobs = (const FoldJob*)ws_jobs.ptr + k;
+      const int nj = (int)kv.second.size();
+      if (mode == PPM_FOLD_BF16X3 && r.tc_ok)
+        PPM_CUDA(fold_tc_launch(r, jobs, nj, nb, B.d_flux, B.d_counts, st));
+      else
+        PPM_CUDA(launch_fold_simt(jobs, nj, r.d_rsp, r.n_ch, r.n_e, nb, B.d_flux, B.d_counts,
+                                  mode != PPM_FOLD_FP32, st));
+      k += nj;
+    }
+  }
+}
+
+IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max) {
+  int ne_t = 1;
+  if (ne_max > 512)
+    ne_t = 4;
+  else if (ne_max > 320)
+    ne_t = 2;
+  if (tune.ne_t > 0 && tune.ne_t * 512 >= ne_max) ne_t = tune.ne_t;
+  int nt = (ne_max + ne_t - 1) / ne_t;
+  nt = (nt + 31) / 32 * 32;
+  nt = std::max(64, std::min(512, nt));
+  int pb = std::min(tune.pb, nt);
+  IntegrandShape s;
+  for (;;) {
+    s = make_shape(nsx_kernel, nt, ne_t, pb, tune.chunk, nf_max, lens.n_cp, lens.n_ca, nsx.nE, nsx.nmu, cells_max);
+    if (s.total <= 200 * 1024 || pb <= 4) break;
+    pb /= 2;
+  }
+  s.bb_fp64 = bb_fp64 ? 1 : 0;
+  return s;
+}
+
+void Engine::collect(const Batch& B, int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info,
+                     cudaStream_t st) {
+  if (flux) {
+    h_out.reserve(sizeof(double) * (size_t)B.flux_off[n]);
+    PPM_CUDA(cudaMemcpyAsync(h_out.ptr, B.d_flux, sizeof(double) * (size_t)B.flux_off[n], cudaMemcpyDeviceToHost, st));
+  }
+  std::vector<unsigned long long> stats((size_t)kStats * n);
+  PPM_CUDA(cudaMemcpyAsync(stats.data(), B.d_stats, sizeof(unsigned long long) * stats.size(), cudaMemcpyDeviceToHost,
+                           st));
+  int ctrl[16];
+  PPM_CUDA(cudaMemcpyAsync(ctrl, ws_ctrl.ptr, sizeof(ctrl), cudaMemcpyDeviceToHost, st));
+  PPM_CUDA(cudaStreamSynchronize(st));
+  if (ctrl[2] || ctrl[5] || ctrl[8]) throw Error(PPM_E_RANGE, "work queue overflow");
+  if (flux) std::memcpy(flux, h_out.ptr, sizeof(double) * (size_t)B.flux_off[n]);
+  if (counts && B.counts_off[n] > 0) {
+    PPM_CUDA(cudaMemcpy(counts, B.d_counts, sizeof(double) * (size_t)B.counts_off[n], cudaMemcpyDeviceToHost));
+  }
+  if (info) {
+    for (int i = 0; i < n; ++i) {
+      ppm_result_info& r = info[i];
+      r.n_active = (int64_t)stats[kStats * i + 0];
+      r.n_rings = (int64_t)stats[kStats * i + 1];
+      r.n_dropped_rings = (int64_t)stats[kStats * i + 2];
+      r.n_points = (int64_t)stats[kStats * i + 3];
+      r.n_clamped = (int64_t)stats[kStats * i + 4];
+      r.status = PPM_OK;
+      r.reserved = 0;
+    }
+  }
+}
+
+void Engine::profile(const ppm_params& p, double* flux, double* counts, ppm_result_info* info) {
+  std::lock_guard<std::mutex> lk(mu);
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  if (counts && p.response < 0) throw Error(PPM_E_INVALID, "counts requested without a response");
+  Batch B;
+  run(1, &p, nullptr, nullptr, B, stream);
+  collect(B, 1, &p, flux, counts, info, stream);
+}
+
+void Engine::profile_batch(int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info) {
+  if (n < 1) throw Error(PPM_E_INVALID, "empty batch");
+  if (n > cfg.max_batch) throw Error(PPM_E_RANGE, "batch larger than max_batch");
+  std::lock_guard<std::mutex> lk(mu);
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  Batch B;
+  run(n, ps, nullptr, nullptr, B, stream);
+  collect(B, n, ps, flux, counts, info, stream);
+}
+
+// Device-resident form: outputs land in caller device buffers, nothing is synchronised.
+void Engine::profile_batch_device(int n, const ppm_params* ps, double* flux_d, double* counts_d, cudaStream_t st) {
+  if (n < 1) throw Error(PPM_E_INVALID, "empty batch");
+  if (!flux_d) throw Error(PPM_E_INVALID, "flux_device is required");
+  std::lock_guard<std::mutex> lk(mu);
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  Batch B;
+  run(n, ps, flux_d, counts_d, B, st ? st : stream);
+}
+
+void Engine::output_sizes(const ppm_params& p, int64_t* n_flux, int64_t* n_counts) const {
+  validate(p);
+  if (n_flux) *n_flux = (int64_t)p.n_bins * (int64_t)grids[p.energy_grid].E.size();
+  if (n_counts) *n_counts = p.response >= 0 ? (int64_t)p.n_bins * resps[p.response].n_ch : 0;
+}
+
+}  // namespace ppm

@@ -1,0 +1,150 @@
+// Engine state shared by the host translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/ppm.h"
+#include "kernels.cuh"
+
+namespace ppm {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t cap = 0;
+  void reserve(size_t bytes);
+  void release();
+};
+
+struct HostBuffer {
+  void* ptr = nullptr;
+  size_t cap = 0;
+  void reserve(size_t bytes);
+  void release();
+};
+
+struct Grid {
+  std::vector<double> E;
+  double* dE = nullptr;
+  double* dinvE = nullptr;
+  int* drE = nullptr;
+  float* dfE = nullptr;
+  int iE_min = 0, span = 1;
+  double tE_lo = 0, tE_hi = 0;
+  int nsx_version = -1;
+};
+
+struct Resp {
+  int grid = 0, n_ch = 0, n_e = 0;
+  double* d_rsp = nullptr;
+  std::vector<double> h_rsp;
+  // tensor-core fold operands: BF16 hi/lo split of rsp, zero padded, in the UMMA core-matrix layout
+  bool tc_ok = false;
+  int m_pad = 0, k_pad = 0;
+  void* d_a_hi = nullptr;
+  void* d_a_lo = nullptr;
+};
+
+struct Batch {
+  int n = 0;
+  std::vector<long long> flux_off, counts_off;
+  double* d_flux = nullptr;
+  double* d_counts = nullptr;
+  unsigned long long* d_stats = nullptr;
+};
+
+struct Tuning {
+  int pb = 32;       // phase points per batch
+  int chunk = 1024;  // candidate elements per tile
+  int ne_t = 0;      // energies per thread (0 = automatic)
+};
+
+struct GraphEntry {
+  cudaGraphExec_t exec = nullptr;
+};
+
+struct Ticket;
+
+class Engine {
+ public:
+  explicit Engine(const ppm_engine_config& c);
+  ~Engine();
+
+  void load_lensing(const ppm_lensing_desc& d);
+  void load_nsx(const ppm_nsx_desc& d);
+  int add_grid(int n_e, const double* E);
+  int add_response(int grid, int n_ch, const double* rsp);
+
+  void profile(const ppm_params& p, double* flux, double* counts, ppm_result_info* info);
+  void profile_batch(int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info);
+  void profile_batch_device(int n, const ppm_params* ps_host, double* flux_d, double* counts_d, cudaStream_t st);
+  void output_sizes(const ppm_params& p, int64_t* n_flux, int64_t* n_counts) const;
+
+  // serving
+  uint64_t submit(const ppm_params& p, double* flux, double* counts);
+  int poll(uint64_t t);
+  int wait(uint64_t t, int timeout_ms, ppm_result_info* info);
+  double latency_us(uint64_t t);
+  void serve_shutdown();
+
+  ppm_engine_config cfg;
+  Tuning tune;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+
+ private:
+  friend struct Server;
+  void validate(const ppm_params& p) const;
+  void to_device(const ppm_params& p, DevProfile& d, long long flux_off, unsigned long long* stats);
+  void prepare_grid(int id);
+  DevGrid dev_grid(int id);
+  const double* ring_table(int N);
+  const double* fine_table(int nf);
+  long long tile_bound(const ppm_params& p, int chunk);
+  IntegrandShape choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max);
+  void run(int n, const ppm_params* ps, double* ext_flux, double* ext_counts, Batch& B, cudaStream_t st);
+  void collect(const Batch& B, int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info,
+               cudaStream_t st);
+  void fold_tc_prepare(Resp& r);
+  cudaError_t fold_tc_launch(const Resp& r, const FoldJob* jobs, int n_jobs, int n_bins, const double* flux,
+                             double* counts, cudaStream_t st);
+  void track(void* p);
+
+  std::mutex mu;
+  bool has_lens = false, has_nsx = false;
+  int nsx_version = 0;
+  DevLens lens{};
+  DevNsx nsx{};
+  std::vector<double> nsx_mu;
+  std::vector<Grid> grids;
+  std::vector<Resp> resps;
+  std::map<int, double*> ring_tabs, fine_tabs;
+  std::map<int, std::vector<double>> host_rings;
+  std::vector<void*> owned;
+  DeviceBuffer ws_prof, ws_flux, ws_counts, ws_stats, ws_tiles, ws_ctrl, ws_jobs;
+  HostBuffer h_stage, h_out;
+  std::vector<FoldJob> h_jobs;
+  std::map<std::string, GraphEntry> graphs;
+  cudaEvent_t ev[3];
+
+  // serving state
+  struct Server* server = nullptr;
+};
+
+}  // namespace ppm

@@ -1,0 +1,856 @@
+// Engine kernels: work planner, persistent integrand (NSX FP32 and blackbody
+// FP64/FP32 variants) and SIMT response folds.
+//
+// Integrand structure (one CTA per tile = candidate elements of one ring of
+// one spot of one profile; CTAs pull tiles from a device queue):
+//   1. ring geometry                      cpu/devarshi24st_cpu.cpp:90-124
+//   2. active-element compaction by warp ballot + prefix (deterministic order)
+//                                         gpu/devarshi24st_gpu.cu:196-212
+//   3. two lensing rows of each table staged in shared memory, FP64 sweep of
+//      the fine phases                    cpu/devarshi24st_cpu.cpp:126-193
+//   4. gap fill / wrap                    cpu/devarshi24st_cpu.cpp:195-212
+//   5. NSX (logT, logg) slice pre-reduced into shared memory (FP32)
+//                                         gpu/devarshi24st_gpu.cu:323-351
+//   6. deposit: batches of phase points (FP64 phase, hunt, lerps); for each
+//      point the mu-contracted slice is turned into per-cell cubic
+//      polynomials in log(E/kT); every thread owns fixed energies and keeps
+//      per-bin partial sums in registers (no per-element atomics); a bin's
+//      partial sums are flushed once into the FP64 flux pool
+//                                         cpu/devarshi24st_cpu.cpp:214-241
+#include <cstdio>
+
+#include "kernels.cuh"
+
+namespace ppm {
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kTwoPi = 2. * kPi;
+constexpr int kSlotBytes = 48;  // bytes per batch point (SoA)
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Block-wide ordered compaction: returns this thread's slot among flagged
+// threads (or -1) and the total through *total.  Uses scratch[32].
+__device__ __forceinline__ int block_compact(bool flag, int* scratch, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  unsigned b = __ballot_sync(0xffffffffu, flag);
+  if (lane == 0) scratch[warp] = __popc(b);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int w = 0; w < nw; ++w) {
+      int c = scratch[w];
+      scratch[w] = run;
+      run += c;
+    }
+    scratch[32] = run;
+  }
+  __syncthreads();
+  int pos = flag ? scratch[warp] + __popc(b & lanemask_lt()) : -1;
+  *total = scratch[32];
+  return pos;
+}
+
+struct SmemPtrs {
+  int* j;
+  double *P, *F, *Z, *MU, *mu;
+  float* S;
+  double* rows;
+  unsigned char* batch;
+  float4* Q;
+  float* H;
+};
+
+__device__ __forceinline__ SmemPtrs carve(unsigned char* sm, const IntegrandShape& S) {
+  SmemPtrs s;
+  s.j = (int*)(sm + S.off_j);
+  s.P = (double*)(sm + S.off_P);
+  s.F = (double*)(sm + S.off_F);
+  s.Z = (double*)(sm + S.off_Z);
+  s.MU = (double*)(sm + S.off_MU);
+  s.mu = (double*)(sm + S.off_mu);
+  s.S = (float*)(sm + S.off_S);
+  s.rows = (double*)(sm + S.off_rows);
+  s.batch = sm + S.off_batch;
+  s.Q = (float4*)(sm + S.off_Q);
+  s.H = (float*)(sm + S.off_Q + (S.nsx ? S.pb * S.cells * 16 : 0));
+  return s;
+}
+
+// Steps 1-4 for one tile.  Returns the number of active elements (0 = nothing to do).
+// On return (non-zero), P/F/Z/MU hold the filled fine-phase arrays and s_g the ring geometry.
+__device__ int tile_prologue(const KernelArgs& a, const DevProfile& p, const DevSpot& sp, const Tile& tile,
+                             const SmemPtrs& s, RingGeom& s_g, int* s_int, bool nsx) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const bool point = sp.kind == 1;
+  const DevLens& L = a.lens;
+  if (tid == 0) {
+    double cos_t = point ? sp.cos_theta_pt : p.ring[3 * tile.ring];
+    double dOmega = point ? sp.dOmega_pt : p.dOmega_hp;
+    ring_geometry(p, L, cos_t, dOmega, nsx, s_g);
+  }
+  // compaction of active elements over the candidate range
+  int n_act = 0;
+  if (point) {
+    if (tid == 0) s.j[0] = 0;
+    n_act = 1;
+  } else {
+    const int N = p.n_side, ring = tile.ring;
+    const double c2 = p.ring[3 * ring + 1], s2 = p.ring[3 * ring + 2];
+    const int n_c = tile.j1 - tile.j0;
+    for (int k0 = 0; k0 < n_c; k0 += nt) {
+      int k = k0 + tid;
+      bool flag = false;
+      if (k < n_c) flag = in_spot(sp, c2, s2, healpix_phi(N, ring, tile.j0 + k));
+      int tot;
+      int pos = block_compact(flag, s_int, &tot);
+      if (flag) s.j[n_act + pos] = tile.j0 + k;
+      n_act += tot;
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  if (n_act == 0) return 0;
+  if (tid == 0) {
+    atomicAdd(&p.stats[0], (unsigned long long)n_act);
+    atomicAdd(&p.stats[1], 1ull);
+    if (s_g.u_clamped && tile.first) atomicAdd(&p.stats[4], 1ull);
+    s_int[40] = p.n_fine + 1;  // invisible min
+    s_int[41] = -1;            // invisible max
+  }
+  // stage the two lensing rows of each table
+  const int ncp = L.n_cp, nca = L.n_ca, iu = s_g.i_u;
+  double* r = s.rows;
+  for (int k = tid; k < 2 * ncp; k += nt) {
+    int row = k / ncp, col = k - row * ncp;
+    r[k] = L.ca[(size_t)(iu + row) * ncp + col];
+    r[2 * ncp + k] = L.lf[(size_t)(iu + row) * ncp + col];
+  }
+  for (int k = tid; k < 2 * nca; k += nt) {
+    int row = k / nca, col = k - row * nca;
+    r[4 * ncp + k] = L.cdt[(size_t)(iu + row) * nca + col];
+  }
+  __syncthreads();
+  LensRows rows{r, r + ncp, r + 2 * ncp, r + 3 * ncp, r + 4 * ncp, r + 4 * ncp + nca};
+  const RingGeom g = s_g;
+  const int nf = p.n_fine;
+  for (int i = tid; i < nf; i += nt) {
+    double F, Z, P, MU;
+    if (sweep_sample(p, L, g, rows, i, nsx, F, Z, P, MU)) {
+      s.F[i] = F;
+      s.Z[i] = Z;
+      s.P[i] = P;
+      s.MU[i] = MU;
+    } else {
+      s.F[i] = 0;
+      s.Z[i] = -1;
+      s.P[i] = -1;
+      s.MU[i] = 0;
+      atomicMin(&s_int[40], i);
+      atomicMax(&s_int[41], i);
+    }
+  }
+  __syncthreads();
+  const int inv_min = s_int[40], inv_max = s_int[41];
+  if (inv_min == 0 || inv_max == nf - 1) return 0;  // cpu/devarshi24st_cpu.cpp:195
+  if (inv_min <= inv_max) {
+    const int beg = inv_min - 1, end = inv_max + 1;
+    const double p0 = s.P[beg], p1 = s.P[end], z0 = s.Z[beg], z1 = s.Z[end];
+    for (int i = inv_min + tid; i <= inv_max; i += nt) {
+      s.P[i] = p0 + (p1 - p0) * ((double)(i - beg) / (end - beg));
+      s.Z[i] = z0 + (z1 - z0) * ((double)(i - beg) / (end - beg));
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    s.F[nf] = s.F[0];
+    s.Z[nf] = s.Z[0];
+    s.P[nf] = 1.0 + s.P[0];
+    s.MU[nf] = s.MU[0];
+  }
+  __syncthreads();
+  return n_act;
+}
+
+// Phase point q of the tile: GL node (or sample phase), patch phase, hunt and
+// lerps in FP64 (cpu/devarshi24st_cpu.cpp:214-229).  Returns flux/I (0 = skip).
+__device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtrs& s, int ring, bool point, int n_act,
+                                              int q, int& bin, double& wgl, double& z, double& mu) {
+  const int n_gl = p.n_gl;
+  const int i_pp = q / n_act, jj = q - i_pp * n_act;
+  int g = 0;
+  if (n_gl > 0) {
+    bin = i_pp / n_gl;
+    g = i_pp - bin * n_gl;
+  } else {
+    bin = i_pp;
+  }
+  const double phi = point ? 0.0 : healpix_phi(p.n_side, ring, s.j[jj]);
+  const double phase_shift = phi / kTwoPi;
+  double ppt;
+  if (n_gl > 0) {
+    const double width = 1. / p.n_bins;
+    const double lb = bin * width, ub = (bin + 1) * width;
+    ppt = 0.5 * (lb + ub + c_gl_nodes[n_gl * (n_gl - 1) / 2 + g] * (ub - lb));
+    wgl = 0.5 * 1. * c_gl_weights[n_gl * (n_gl - 1) / 2 + g];
+  } else {
+    ppt = bin * (1.0 / p.n_bins);
+    wgl = 1.0;
+  }
+  double patch = fmod(ppt + phase_shift + 1., 1.);
+  if (patch < s.P[0]) patch += 1.;
+  double af;
+  const int i = vhunt(s.P, p.n_fine + 1, patch, af);
+  const double flux = (1 - af) * s.F[i] + af * s.F[i + 1];
+  if (flux == 0) return 0.0;
+  z = (1 - af) * s.Z[i] + af * s.Z[i + 1];
+  mu = (1 - af) * s.MU[i] + af * s.MU[i + 1];
+  return flux;
+}
+
+// ---------------------------------------------------------------------------
+template <int NE_T>
+__global__ void __launch_bounds__(512) integrand_nsx_kernel(const KernelArgs a) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  const IntegrandShape& S = a.shape;
+  const SmemPtrs s = carve(sm, S);
+  __shared__ RingGeom s_g;
+  __shared__ int s_int[48];
+  __shared__ int s_tile;
+  __shared__ float s_tapw[16];
+  __shared__ int s_tapo[16];
+  __shared__ int s_ntap;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const DevNsx& X = a.nsx;
+  const int nE = X.nE, nmu = X.nmu, cells = S.cells, HN = cells + 3;
+
+  // batch SoA
+  float* b_c = (float*)s.batch;
+  float* b_fP = b_c + S.pb;
+  int* b_G0 = (int*)(b_fP + S.pb);
+  int* b_bin = b_G0 + S.pb;
+  int* b_imu = b_bin + S.pb;
+  float* b_w = (float*)(b_imu + S.pb);  // [4][pb]
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_tile = atomicAdd(a.queue.next, 1);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= *a.queue.n_tiles || t >= a.queue.capacity) break;
+    const Tile tile = a.queue.tiles[t];
+    const DevProfile& p = a.profiles[tile.profile];
+    const DevSpot& sp = p.spot[tile.spot];
+    const bool point = sp.kind == 1;
+    const int n_act = tile_prologue(a, p, sp, tile, s, s_g, s_int, true);
+    if (n_act == 0) continue;
+
+    // ---- step 5: (logT, logg) pre-reduction of the NSX table into S[E][mu]
+    if (tid == 0) {
+      const bool cubic = (p.interp == 0 || p.interp == 1 || p.interp == 2);
+      double lg = s_g.logg, ag;
+      s_int[45] = (lg < X.g_min || lg > X.g_max) ? 1 : 0;
+      s_int[44] = 0;
+      int ig = uhunt(lg, X.g_min, X.g_max, X.ng, ag);
+      double wg[4];
+      int ig0, ngt;
+      if (cubic) {
+        ig0 = clampi(ig - 1, 0, X.ng - 4);
+        cubic_lagrange(wg, lg, uhunt_at(X.g_min, X.g_max, X.ng, ig0), uhunt_at(X.g_min, X.g_max, X.ng, ig0 + 1),
+                       uhunt_at(X.g_min, X.g_max, X.ng, ig0 + 2), uhunt_at(X.g_min, X.g_max, X.ng, ig0 + 3));
+        ngt = 4;
+      } else {
+        ig0 = ig;
+        wg[0] = 1 - ag;
+        wg[1] = ag;
+        ngt = 2;
+      }
+      int n = 0;
+      for (int jt = 0; jt < sp.nT_taps; ++jt)
+        for (int jg = 0; jg < ngt; ++jg) {
+          s_tapw[n] = (float)(sp.wT[jt] * wg[jg]);
+          s_tapo[n] = (sp.iT[jt] * X.ng + ig0 + jg) * X.slice_stride;
+          ++n;
+        }
+      s_ntap = n;
+    }
+    for (int k = tid; k < nmu; k += nt) s.mu[k] = X.mu[k];
+    __syncthreads();
+    {
+      const int n4 = X.slice_stride >> 2, ntap = s_ntap;
+      float4* S4 = (float4*)s.S;
+      for (int k = tid; k < n4; k += nt) {
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int q = 0; q < ntap; ++q) {
+          const float4 v = __ldg((const float4*)(X.data + s_tapo[q]) + k);
+          const float w = s_tapw[q];
+          acc.x = fmaf(w, v.x, acc.x);
+          acc.y = fmaf(w, v.y, acc.y);
+          acc.z = fmaf(w, v.z, acc.z);
+          acc.w = fmaf(w, v.w, acc.w);
+        }
+        S4[k] = acc;
+      }
+    }
+    __syncthreads();
+
+    // ---- step 6: deposit
+    const DevGrid& G = p.grid;
+    const int n_e = G.n_e;
+    int rE[NE_T];
+    float fE[NE_T];
+    float acc[NE_T];
+#pragma unroll
+    for (int k = 0; k < NE_T; ++k) {
+      const int e = tid + k * nt;
+      const bool ok = e < n_e;
+      rE[k] = ok ? G.rE[e] : 0;
+      fE[k] = ok ? G.fE[e] : 0.f;
+      acc[k] = 0.f;
+    }
+    const int mode = p.interp;
+    const bool cubicE = mode != 4;
+    const bool sg = mode == 1;
+    const double mu_min = s.mu[nmu - 1];
+    const int n_pp = p.n_gl > 0 ? p.n_bins * p.n_gl : p.n_bins;
+    const int n_pts = n_pp * n_act;
+    int cur_bin = -1;
+    double* flux_base = a.flux + p.flux_off;
+    const double out_scale = sp.out_scale;
+
+    auto flush = [&]() {
+#pragma unroll
+      for (int k = 0; k < NE_T; ++k) {
+        const int e = tid + k * nt;
+        if (e < n_e && acc[k] != 0.f)
+          atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)acc[k] * out_scale * G.invE[e]);
+        acc[k] = 0.f;
+      }
+    };
+
+    for (int q0 = 0; q0 < n_pts; q0 += S.pb) {
+      // stage A: phase points -> batch (visible ones, order kept)
+      bool vis = false, clamped = false;
+      float c = 0.f, fP = 0.f;
+      int G0 = 0, bin = 0, imu = 0;
+      float w4[4] = {0.f, 0.f, 0.f, 0.f};
+      const int q = q0 + tid;
+      if (tid < S.pb && q < n_pts) {
+        double wgl, z = 0, mu = 0;
+        const double flux = phase_point(p, s, tile.ring, point, n_act, q, bin, wgl, z, mu);
+        if (flux != 0.0) {
+          vis = true;
+          if (mu < mu_min) mu = mu_min;
+          c = (float)(flux * wgl);
+          const double tP = (log10(z) - sp.l10kT - X.E_min) * X.inv_dE;
+          const double fl = floor(tP);
+          fP = (float)(tP - fl);
+          G0 = G.iE_min + (int)fl;
+          clamped = (G.tE_lo + tP < 0.0) || (G.tE_hi + tP > (double)(nE - 1)) || sp.T_clamped || s_int[45];
+          // mu weights (cpu/nsx.hpp:173-321)
+          double am;
+          const int im = vhunt(s.mu, nmu, mu, am);
+          double w[4] = {0, 0, 0, 0};
+          int start;
+          const bool linear_mu = (mode == 4) || ((mode == 2 || mode == 3) && im >= nmu - 5);
+          if (linear_mu) {
+            start = min(im, nmu - 4);
+            const int o = im - start;
+            w[o] = 1 - am;
+            w[o + 1] = am;
+          } else {
+            start = clampi(im - 1, 0, nmu - 4);
+            cubic_lagrange(w, mu, s.mu[start], s.mu[start + 1], s.mu[start + 2], s.mu[start + 3]);
+          }
+          imu = start;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) w4[k] = (float)w[k];
+        }
+      }
+      int n_batch;
+      const int slot = block_compact(vis, s_int, &n_batch);
+      if (vis) {
+        b_c[slot] = c;
+        b_fP[slot] = fP;
+        b_G0[slot] = G0;
+        b_bin[slot] = bin;
+        b_imu[slot] = imu;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) b_w[k * S.pb + slot] = w4[k];
+      }
+      if (vis && clamped) atomicAdd(&s_int[44], 1);
+      __syncthreads();
+      if (tid == 0) {
+        if (n_batch) atomicAdd(&p.stats[3], (unsigned long long)n_batch);
+        if (s_int[44]) atomicAdd(&p.stats[4], (unsigned long long)s_int[44]);
+        s_int[44] = 0;
+      }
+      __syncthreads();
+      if (n_batch == 0) continue;
+
+      // stage B1: mu-contracted slice rows H[b][kk], k = kH0 + kk
+      for (int idx = tid; idx < n_batch * HN; idx += nt) {
+        const int b = idx / HN, kk = idx - b * HN;
+        const int kH0 = clampi(b_G0[b] - 1, 0, nE - 4);
+        const int k = kH0 + kk;
+        float h = 0.f;
+        if (k < nE) {
+          const float* row = s.S + k * nmu + b_imu[b];
+          h = b_w[b] * row[0];
+          h = fmaf(b_w[S.pb + b], row[1], h);
+          h = fmaf(b_w[2 * S.pb + b], row[2], h);
+          h = fmaf(b_w[3 * S.pb + b], row[3], h);
+        }
+        s.H[idx] = h;
+      }
+      __syncthreads();
+      // stage B2: per-cell polynomials in the cell fraction
+      for (int idx = tid; idx < n_batch * cells; idx += nt) {
+        const int b = idx / cells, cc = idx - b * cells;
+        const int G0b = b_G0[b];
+        const int kH0 = clampi(G0b - 1, 0, nE - 4);
+        const float* H = s.H + b * HN;
+        const int gcell = G0b + cc;
+        float4 Q;
+        if (gcell < 0) {
+          Q = make_float4(H[0 - kH0], 0.f, 0.f, 0.f);
+        } else if (gcell > nE - 2) {
+          Q = make_float4(H[nE - 1 - kH0], 0.f, 0.f, 0.f);
+        } else if (cubicE) {
+          const int ie = clampi(gcell - 1, 0, nE - 4);
+          const int off = gcell - ie;
+          const float h0 = H[ie - kH0], h1 = H[ie - kH0 + 1], h2 = H[ie - kH0 + 2], h3 = H[ie - kH0 + 3];
+          const float d1 = h1 - h0, d2 = h2 - 2.f * h1 + h0, d3 = h3 - 3.f * h2 + 3.f * h1 - h0;
+          const float c3 = d3 * (1.f / 6.f);
+          if (off == 1)
+            Q = make_float4(h1, d1 + 0.5f * d2 - c3, 0.5f * d2, c3);
+          else if (off == 0)
+            Q = make_float4(h0, d1 - 0.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 - 0.5f * d3, c3);
+          else
+            Q = make_float4(h2, d1 + 1.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 + 0.5f * d3, c3);
+        } else {
+          const float h0 = H[gcell - kH0], h1 = H[gcell - kH0 + 1];
+          Q = make_float4(h0, h1 - h0, 0.f, 0.f);
+        }
+        s.Q[idx] = Q;
+      }
+      __syncthreads();
+
+      // stage C: every thread integrates its energies over the batch
+      for (int b = 0; b < n_batch; ++b) {
+        const int bb = b_bin[b];
+        if (bb != cur_bin) {
+          if (cur_bin >= 0) flush();
+          cur_bin = bb;
+        }
+        const float cb = b_c[b], fPb = b_fP[b];
+        const float4* Qb = s.Q + b * cells;
+#pragma unroll
+        for (int k = 0; k < NE_T; ++k) {
+          float tf = fE[k] + fPb;
+          int cidx = rE[k];
+          if (tf >= 1.f) {
+            tf -= 1.f;
+            cidx += 1;
+          }
+          const float4 Qv = Qb[cidx];
+          float it3 = fmaf(fmaf(fmaf(Qv.w, tf, Qv.z), tf, Qv.y), tf, Qv.x);
+          if (sg) it3 = fmaxf(it3, 0.f);
+          acc[k] = fmaf(cb, it3, acc[k]);
+        }
+      }
+    }
+    if (cur_bin >= 0) flush();
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <typename Real, int NE_T>
+__global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  const IntegrandShape& S = a.shape;
+  const SmemPtrs s = carve(sm, S);
+  __shared__ RingGeom s_g;
+  __shared__ int s_int[48];
+  __shared__ int s_tile;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double* b_c = (double*)s.batch;
+  double* b_z = b_c + S.pb;
+  int* b_bin = (int*)(b_z + S.pb);
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_tile = atomicAdd(a.queue.next, 1);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= *a.queue.n_tiles || t >= a.queue.capacity) break;
+    const Tile tile = a.queue.tiles[t];
+    const DevProfile& p = a.profiles[tile.profile];
+    const DevSpot& sp = p.spot[tile.spot];
+    const bool point = sp.kind == 1;
+    const int n_act = tile_prologue(a, p, sp, tile, s, s_g, s_int, false);
+    if (n_act == 0) continue;
+
+    const DevGrid& G = p.grid;
+    const int n_e = G.n_e;
+    Real E[NE_T], acc[NE_T];
+#pragma unroll
+    for (int k = 0; k < NE_T; ++k) {
+      const int e = tid + k * nt;
+      E[k] = e < n_e ? (Real)G.E[e] : (Real)1;
+      acc[k] = 0;
+    }
+    const Real kT = (Real)sp.kT;
+    const int n_pp = p.n_gl > 0 ? p.n_bins * p.n_gl : p.n_bins;
+    const int n_pts = n_pp * n_act;
+    int cur_bin = -1;
+    double* flux_base = a.flux + p.flux_off;
+    const double out_scale = sp.out_scale;
+    auto flush = [&]() {
+#pragma unroll
+      for (int k = 0; k < NE_T; ++k) {
+        const int e = tid + k * nt;
+        if (e < n_e && acc[k] != (Real)0)
+          atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)acc[k] * out_scale * G.invE[e]);
+        acc[k] = 0;
+      }
+    };
+    for (int q0 = 0; q0 < n_pts; q0 += S.pb) {
+      bool vis = false;
+      double c = 0, zz = 0;
+      int bin = 0;
+      const int q = q0 + tid;
+      if (tid < S.pb && q < n_pts) {
+        double wgl, z = 0, mu = 0;
+        const double flux = phase_point(p, s, tile.ring, point, n_act, q, bin, wgl, z, mu);
+        if (flux != 0.0) {
+          vis = true;
+          c = flux * wgl;
+          zz = z;
+        }
+      }
+      int n_batch;
+      const int slot = block_compact(vis, s_int, &n_batch);
+      if (vis) {
+        b_c[slot] = c;
+        b_z[slot] = zz;
+        b_bin[slot] = bin;
+      }
+      if (tid == 0 && n_batch) atomicAdd(&p.stats[3], (unsigned long long)n_batch);
+      __syncthreads();
+      for (int b = 0; b < n_batch; ++b) {
+        const int bb = b_bin[b];
+        if (bb != cur_bin) {
+          if (cur_bin >= 0) flush();
+          cur_bin = bb;
+        }
+        const Real cb = (Real)b_c[b], zb = (Real)b_z[b];
+#pragma unroll
+        for (int k = 0; k < NE_T; ++k) {
+          // Ibb(E, kT) = Ibb_constant E^3 / expm1(E / kT) (cpu/unit.hpp:28-31); the constant is in out_scale
+          const Real Ee = E[k] * zb;
+          const Real I = Ee * Ee * Ee / expm1(Ee / kT);
+          acc[k] += cb * I;
+        }
+      }
+      __syncthreads();
+    }
+    if (cur_bin >= 0) flush();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ring range of disk 1 in element index j: up to two [j_lo, j_hi] ranges
+// (with a one-element margin) that contain every active element.
+__device__ int candidate_ranges(const DevSpot& s, int N, int i, double c2, double s2, int jmax, int r[2][2]) {
+  const double A = s.s1 * s2, B = s.c1 * c2;
+  bool full = false;
+  double w = 0.0;
+  if (A < 1e-12) {
+    if (B > s.cos_ar1 - 1e-9)
+      full = true;
+    else
+      return 0;
+  } else {
+    const double qv = (s.cos_ar1 - B) / A;
+    if (qv > 1.0 + 1e-9) return 0;
+    if (qv <= -1.0)
+      full = true;
+    else
+      w = acos(fmin(qv, 1.0)) + 1e-7;
+    if (w >= kPi) full = true;
+  }
+  if (full) {
+    r[0][0] = 1;
+    r[0][1] = jmax;
+    return 1;
+  }
+  const int ii = i > 2 * N ? 4 * N - i : i;
+  const double sh = ii < N ? 0.5 : 0.5 * ((ii - N + 1) % 2);
+  const double dphi = kTwoPi / jmax;
+  const double jc = s.ph1 / dphi + sh, jw = w / dphi;
+  long long jlo = (long long)floor(jc - jw) - 1, jhi = (long long)ceil(jc + jw) + 1;
+  const long long len = jhi - jlo + 1;
+  if (len >= jmax) {
+    r[0][0] = 1;
+    r[0][1] = jmax;
+    return 1;
+  }
+  long long m = ((jlo - 1) % jmax + jmax) % jmax + 1;  // jlo mapped into [1, jmax]
+  if (m + len - 1 <= jmax) {
+    r[0][0] = (int)m;
+    r[0][1] = (int)(m + len - 1);
+    return 1;
+  }
+  r[0][0] = (int)m;
+  r[0][1] = jmax;
+  r[1][0] = 1;
+  r[1][1] = (int)(m + len - 1 - jmax);
+  return 2;
+}
+
+// Whether the ring is skipped because fine sample 0 or n_fine-1 is invisible
+// (cpu/devarshi24st_cpu.cpp:195), evaluated with the sweep's own arithmetic.
+__device__ bool ring_dropped(const DevProfile& p, const DevLens& L, const RingGeom& g, bool nsx) {
+  LensRows rows;
+  lens_rows_global(L, g.i_u, rows);
+  double F, Z, P, MU;
+  if (!sweep_sample(p, L, g, rows, 0, nsx, F, Z, P, MU)) return true;
+  if (!sweep_sample(p, L, g, rows, p.n_fine - 1, nsx, F, Z, P, MU)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void push_tile(const WorkQueue& q, const Tile& t) {
+  const int k = atomicAdd(q.n_tiles, 1);
+  if (k < q.capacity)
+    q.tiles[k] = t;
+  else
+    atomicOr(q.overflow, 1);
+}
+
+__global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const DevLens L, const WorkQueue q, int chunk) {
+  const int pi = blockIdx.x / kMaxSpots, si = blockIdx.x % kMaxSpots;
+  if (pi >= n_profiles) return;
+  const DevProfile& p = profiles[pi];
+  if (si >= p.n_spots) return;
+  const DevSpot& sp = p.spot[si];
+  const bool nsx = p.atmosphere == 0;
+  if (sp.kind == 1) {
+    if (threadIdx.x == 0) {
+      RingGeom g;
+      ring_geometry(p, L, sp.cos_theta_pt, sp.dOmega_pt, false, g);
+      if (ring_dropped(p, L, g, nsx)) {
+        atomicAdd(&p.stats[1], 1ull);
+        atomicAdd(&p.stats[2], 1ull);
+        atomicAdd(&p.stats[0], 1ull);
+      } else {
+        push_tile(q, Tile{pi, (short)si, 1, 0, 0, 1});
+      }
+    }
+    return;
+  }
+  const int N = p.n_side;
+  for (int i = sp.i_lo + threadIdx.x; i <= sp.i_hi; i += blockDim.x) {
+    const double z = p.ring[3 * i], c2 = p.ring[3 * i + 1], s2 = p.ring[3 * i + 2];
+    const int jmax = healpix_jmax(N, i);
+    int r[2][2];
+    const int nr = candidate_ranges(sp, N, i, c2, s2, jmax, r);
+    if (nr == 0) continue;
+    RingGeom g;
+    ring_geometry(p, L, z, p.dOmega_hp, false, g);
+    if (ring_dropped(p, L, g, nsx)) {
+      // count the ring (and its elements) only if it holds active elements
+      long long na = 0;
+      for (int k = 0; k < nr; ++k)
+        for (int j = r[k][0]; j <= r[k][1]; ++j) na += in_spot(sp, c2, s2, healpix_phi(N, i, j)) ? 1 : 0;
+      if (na) {
+        atomicAdd(&p.stats[1], 1ull);
+        atomicAdd(&p.stats[2], 1ull);
+        atomicAdd(&p.stats[0], (unsigned long long)na);
+        if (g.u_clamped) atomicAdd(&p.stats[4], 1ull);
+      }
+      continue;
+    }
+    bool first = true;
+    for (int k = 0; k < nr; ++k)
+      for (int j0 = r[k][0]; j0 <= r[k][1]; j0 += chunk) {
+        const int j1 = min(j0 + chunk, r[k][1] + 1);
+        push_tile(q, Tile{pi, (short)si, (short)(first ? 1 : 0), i, j0, j1});
+        first = false;
+      }
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <typename Real>
+__global__ void fold_simt_kernel(const FoldJob* jobs, const double* rsp, int n_ch, int n_e, int n_bins,
+                                 const double* flux, double* counts) {
+  constexpr int TC = 16, TB = 16, TK = 32;
+  __shared__ Real sr[TC][TK + 1];
+  __shared__ Real sf[TB][TK + 1];
+  const FoldJob job = jobs[blockIdx.z];
+  const int c0 = blockIdx.x * TC, b0 = blockIdx.y * TB;
+  const int tx = threadIdx.x % TB, ty = threadIdx.x / TB;  // tx: bin, ty: channel
+  const double* F = flux + job.flux_off;
+  Real acc = 0;
+  for (int k0 = 0; k0 < n_e; k0 += TK) {
+    for (int idx = threadIdx.x; idx < TC * TK; idx += blockDim.x) {
+      const int cc = idx / TK, kk = idx % TK;
+      const int c = c0 + cc, k = k0 + kk;
+      sr[cc][kk] = (c < n_ch && k < n_e) ? (Real)rsp[(size_t)c * n_e + k] : (Real)0;
+    }
+    for (int idx = threadIdx.x; idx < TB * TK; idx += blockDim.x) {
+      const int bb = idx / TK, kk = idx % TK;
+      const int b = b0 + bb, k = k0 + kk;
+      sf[bb][kk] = (b < n_bins && k < n_e) ? (Real)F[(size_t)b * n_e + k] : (Real)0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < TK; ++kk) acc += sr[ty][kk] * sf[tx][kk];
+    __syncthreads();
+  }
+  const int c = c0 + ty, b = b0 + tx;
+  if (c < n_ch && b < n_bins) counts[job.counts_off + (size_t)c * n_bins + b] = (double)acc * job.alpha;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int n_fine, int n_cp, int n_ca, int nE,
+                          int nmu, int cells) {
+  IntegrandShape s{};
+  s.nsx = nsx;
+  s.nt = nt;
+  s.ne_t = ne_t;
+  s.pb = pb;
+  s.max_cand = max_cand;
+  s.n_fine = n_fine;
+  s.n_cp = n_cp;
+  s.n_ca = n_ca;
+  s.nE = nsx ? nE : 0;
+  s.nmu = nsx ? nmu : 0;
+  s.cells = nsx ? cells : 0;
+  auto al = [](long v) { return (int)((v + 15) / 16 * 16); };
+  int off = 0;
+  s.off_j = off;
+  off += al((long)max_cand * 4);
+  const long nf1 = n_fine + 1;
+  s.off_P = off;
+  off += al(nf1 * 8);
+  s.off_F = off;
+  off += al(nf1 * 8);
+  s.off_Z = off;
+  off += al(nf1 * 8);
+  s.off_MU = off;
+  off += al(nf1 * 8);
+  s.off_mu = off;
+  off += nsx ? al((long)nmu * 8) : 0;
+  s.off_S = off;
+  // the slice is stored with the table's 16-byte aligned stride
+  const long slice = nsx ? ((long)nE * nmu + 3) / 4 * 4 : 0;
+  off += al(slice * 4);
+  s.off_union = off;
+  const int rows = al((long)(4 * n_cp + 2 * n_ca) * 8);
+  const int batch = al((long)pb * kSlotBytes);
+  const int qbuf = nsx ? al((long)pb * cells * 16) + al((long)pb * (cells + 3) * 4) : 0;
+  s.off_rows = off;
+  s.off_batch = off;
+  s.off_Q = off + batch;
+  off += rows > batch + qbuf ? rows : batch + qbuf;
+  s.total = off;
+  return s;
+}
+
+namespace {
+template <int NE_T>
+void* nsx_fn() {
+  return (void*)integrand_nsx_kernel<NE_T>;
+}
+void* kernel_for(const IntegrandShape& s, int precision) {
+  if (s.nsx) {
+    switch (s.ne_t) {
+      case 1: return nsx_fn<1>();
+      case 2: return nsx_fn<2>();
+      default: return nsx_fn<4>();
+    }
+  }
+  if (precision == 1) {
+    switch (s.ne_t) {
+      case 1: return (void*)integrand_bb_kernel<double, 1>;
+      case 2: return (void*)integrand_bb_kernel<double, 2>;
+      default: return (void*)integrand_bb_kernel<double, 4>;
+    }
+  }
+  switch (s.ne_t) {
+    case 1: return (void*)integrand_bb_kernel<float, 1>;
+    case 2: return (void*)integrand_bb_kernel<float, 2>;
+    default: return (void*)integrand_bb_kernel<float, 4>;
+  }
+}
+}  // namespace
+
+cudaError_t configure_integrand_smem(const IntegrandShape& s) {
+  // all variants get the largest dynamic shared memory allowance once
+  static bool done = false;
+  if (done) return cudaSuccess;
+  void* fns[] = {(void*)integrand_nsx_kernel<1>, (void*)integrand_nsx_kernel<2>, (void*)integrand_nsx_kernel<4>,
+                 (void*)integrand_bb_kernel<double, 1>, (void*)integrand_bb_kernel<double, 2>,
+                 (void*)integrand_bb_kernel<double, 4>, (void*)integrand_bb_kernel<float, 1>,
+                 (void*)integrand_bb_kernel<float, 2>, (void*)integrand_bb_kernel<float, 4>};
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  for (void* f : fns) {
+    cudaFuncAttributes at{};
+    e = cudaFuncGetAttributes(&at, f);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)at.sharedSizeBytes);
+    if (e != cudaSuccess) return e;
+  }
+  done = true;
+  return cudaSuccess;
+}
+
+int max_active_ctas(const IntegrandShape& s) {
+  int n = 0;
+  void* f = kernel_for(s, s.bb_fp64);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, s.nt, s.total) != cudaSuccess) return 0;
+  return n;
+}
+
+cudaError_t launch_plan(const DevProfile* profiles, int n_profiles, const DevLens& lens, const WorkQueue& q, int chunk,
+                        cudaStream_t st) {
+  if (n_profiles <= 0) return cudaSuccess;
+  plan_kernel<<<n_profiles * kMaxSpots, 128, 0, st>>>(profiles, n_profiles, lens, q, chunk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_integrand(const KernelArgs& a, int grid, cudaStream_t st) {
+  if (grid <= 0) return cudaSuccess;
+  const IntegrandShape& s = a.shape;
+  void* f = nullptr;
+  f = kernel_for(s, s.bb_fp64);
+  void* args[] = {(void*)&a};
+  return cudaLaunchKernel(f, dim3(grid), dim3(s.nt), args, s.total, st);
+}
+
+cudaError_t launch_fold_simt(const FoldJob* jobs, int n_jobs, const double* rsp, int n_ch, int n_e, int n_bins,
+                             const double* flux, double* counts, bool fp64, cudaStream_t st) {
+  if (n_jobs <= 0) return cudaSuccess;
+  dim3 grid((n_ch + 15) / 16, (n_bins + 15) / 16, n_jobs);
+  if (fp64)
+    fold_simt_kernel<double><<<grid, 256, 0, st>>>(jobs, rsp, n_ch, n_e, n_bins, flux, counts);
+  else
+    fold_simt_kernel<float><<<grid, 256, 0, st>>>(jobs, rsp, n_ch, n_e, n_bins, flux, counts);
+  return cudaGetLastError();
+}
+
+}  // namespace ppm

@@ -1,0 +1,52 @@
+// Launch-side declarations of the engine kernels (defined in kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace ppm {
+
+// Shared-memory carve-up of the integrand kernels; host and device compute it
+// from the same inputs so the launch size always matches what the kernel uses.
+struct IntegrandShape {
+  int nt;         // threads per CTA
+  int ne_t;       // energies per thread (1, 2 or 4)
+  int pb;         // phase points per batch
+  int max_cand;   // candidate elements per tile
+  int n_fine;     // largest n_fine among the profiles
+  int n_cp, n_ca; // lensing row lengths
+  int nE, nmu;    // NSX slice
+  int cells;      // Q cells per point (span + 1)
+  bool nsx;
+  int bb_fp64;    // blackbody variant: 1 = FP64 integrand, 0 = FP32
+  // offsets in bytes
+  int off_j, off_P, off_F, off_Z, off_MU, off_mu, off_S, off_union, off_rows, off_batch, off_Q, total;
+};
+
+IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int n_fine, int n_cp, int n_ca, int nE,
+                          int nmu, int cells);
+
+struct KernelArgs {
+  const DevProfile* profiles;
+  DevLens lens;
+  DevNsx nsx;
+  WorkQueue queue;
+  double* flux;  // pool
+  IntegrandShape shape;
+};
+
+cudaError_t launch_plan(const DevProfile* profiles, int n_profiles, const DevLens& lens, const WorkQueue& q, int chunk,
+                        cudaStream_t st);
+cudaError_t launch_integrand(const KernelArgs& a, int grid, cudaStream_t st);
+// counts[c][b] = alpha * sum_E rsp[c][E] * flux[b][E] for each listed profile, FP64 or FP32 SIMT
+struct FoldJob {
+  long long flux_off, counts_off;
+  double alpha;
+};
+cudaError_t launch_fold_simt(const FoldJob* jobs, int n_jobs, const double* rsp, int n_ch, int n_e, int n_bins,
+                             const double* flux, double* counts, bool fp64, cudaStream_t st);
+int max_active_ctas(const IntegrandShape& s);
+cudaError_t configure_integrand_smem(const IntegrandShape& s);
+
+}  // namespace ppm

@@ -1,0 +1,144 @@
+"""Python host layer over libppm_b200.so (include/ppm.h).
+
+`Engine` owns one device's resident tables (lensing, NSX, energy grids,
+responses) and runs profiles through the C ABI:
+
+* `profile(p)`            plain form: one profile, one pass of the kernels
+  (replaces calc_one_star, gpu/devarshi24st_gpu.cu:432-511);
+* `profile_batch(ps)`     batched form: one persistent launch over all profiles;
+* `submit / wait`         serving form (continuous batching).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import check, dptr, lib
+
+
+class Engine:
+    def __init__(self, device=0, max_batch=65536, memory_budget=0, autotune=0, n_streams=4):
+        cfg = _abi.EngineConfig(device, max_batch, memory_budget, autotune, n_streams)
+        h = ctypes.c_void_p()
+        check(lib().ppm_engine_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self.grids = {}      # id -> energies
+        self.responses = {}  # id -> (grid, n_ch)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ppm_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    # ---- tables
+    def load_lensing(self, tables):
+        d = tables.desc()
+        check(lib().ppm_engine_load_lensing(self.h, ctypes.byref(d)))
+
+    def load_lensing_dir(self, path):
+        check(lib().ppm_engine_load_lensing_dir(self.h, str(path).encode()))
+
+    def load_nsx(self, table):
+        d = table.desc()
+        check(lib().ppm_engine_load_nsx(self.h, ctypes.byref(d)))
+
+    def load_nsx_file(self, path, axes):
+        check(lib().ppm_engine_load_nsx_file(self.h, str(path).encode(), ctypes.byref(axes)))
+
+    def add_energy_grid(self, energies):
+        e = np.ascontiguousarray(energies, dtype=np.float64)
+        gid = ctypes.c_int32()
+        check(lib().ppm_engine_add_energy_grid(self.h, len(e), dptr(e), ctypes.byref(gid)))
+        self.grids[gid.value] = e.copy()
+        return gid.value
+
+    def add_response(self, grid, rsp):
+        r = np.ascontiguousarray(rsp, dtype=np.float64)
+        rid = ctypes.c_int32()
+        check(lib().ppm_engine_add_response(self.h, grid, r.shape[0], dptr(r), ctypes.byref(rid)))
+        self.responses[rid.value] = (grid, r.shape[0])
+        return rid.value
+
+    def load_ism_inst_dir(self, path):
+        g = ctypes.c_int32()
+        r = ctypes.c_int32()
+        check(lib().ppm_engine_load_ism_inst_dir(self.h, str(path).encode(), ctypes.byref(g), ctypes.byref(r)))
+        e = np.loadtxt(f"{path}/E_obs.txt", ndmin=1)
+        self.grids[g.value] = e
+        n_ch = int(open(f"{path}/num.txt").read().split()[0])
+        self.responses[r.value] = (g.value, n_ch)
+        return g.value, r.value
+
+    # ---- sizes
+    def sizes(self, p):
+        n_e = len(self.grids[p.energy_grid])
+        n_ch = self.responses[p.response][1] if p.response >= 0 else 0
+        return (p.n_bins, n_e), (n_ch, p.n_bins)
+
+    # ---- profiles
+    def profile(self, p, want_flux=True, want_counts=None):
+        fs, cs = self.sizes(p)
+        if want_counts is None:
+            want_counts = p.response >= 0
+        flux = np.zeros(fs) if want_flux else None
+        counts = np.zeros(cs) if want_counts else None
+        info = _abi.ResultInfo()
+        check(lib().ppm_profile(self.h, ctypes.byref(p), dptr(flux), dptr(counts), ctypes.byref(info)))
+        return flux, counts, info
+
+    def profile_batch(self, plist, want_flux=True, want_counts=None):
+        n = len(plist)
+        arr = (_abi.Params * n)(*plist)
+        fsz = [self.sizes(p) for p in plist]
+        nf = sum(a[0] * a[1] for a, _ in fsz)
+        nc = sum(b[0] * b[1] for _, b in fsz)
+        if want_counts is None:
+            want_counts = nc > 0
+        flux = np.zeros(nf) if want_flux else None
+        counts = np.zeros(max(nc, 1)) if want_counts else None
+        infos = (_abi.ResultInfo * n)()
+        check(lib().ppm_profile_batch(self.h, n, arr, dptr(flux), dptr(counts), infos))
+        out_f, out_c = [], []
+        of = oc = 0
+        for (fa, ca) in fsz:
+            if want_flux:
+                out_f.append(flux[of:of + fa[0] * fa[1]].reshape(fa))
+            if want_counts:
+                out_c.append(counts[oc:oc + ca[0] * ca[1]].reshape(ca) if ca[0] else None)
+            of += fa[0] * fa[1]
+            oc += ca[0] * ca[1]
+        return out_f, out_c, list(infos)
+
+    def profile_batch_device(self, plist, flux_ptr, counts_ptr, stream=0):
+        """Enqueues a batch whose outputs go to device buffers (integer device pointers)."""
+        n = len(plist)
+        arr = (_abi.Params * n)(*plist)
+        check(lib().ppm_profile_batch_device(self.h, n, arr, None, ctypes.c_void_p(flux_ptr),
+                                             ctypes.c_void_p(counts_ptr) if counts_ptr else None,
+                                             ctypes.c_void_p(stream)))
+
+    # ---- serving
+    def submit(self, p, flux, counts):
+        t = ctypes.c_uint64()
+        check(lib().ppm_submit(self.h, ctypes.byref(p), dptr(flux), dptr(counts), ctypes.byref(t)))
+        return t.value
+
+    def poll(self, ticket):
+        d = ctypes.c_int32()
+        check(lib().ppm_poll(self.h, ticket, ctypes.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket, timeout_ms=-1):
+        info = _abi.ResultInfo()
+        check(lib().ppm_wait(self.h, ticket, timeout_ms, ctypes.byref(info)))
+        return info
+
+    def latency_us(self, ticket):
+        v = ctypes.c_double()
+        check(lib().ppm_ticket_latency_us(self.h, ticket, ctypes.byref(v)))
+        return v.value

@@ -1,0 +1,145 @@
+"""Engine (sm_100a kernels, through the C ABI) against the FP64 oracle and the
+reference's own golden vectors.
+
+Tolerances (tests/errors.py metric, floor 1e-6 of the max):
+  * FP32 NSX integrand: 1e-4 relative per bin and per channel;
+  * FP64 blackbody integrand: 1e-6 relative."""
+import numpy as np
+import pytest
+
+import oracle
+from gpu_ppm_b200 import _abi, synth
+from gpu_ppm_b200.engine import Engine
+from tests import golden_cases as gc
+from tests.errors import max_rel
+
+pytestmark = pytest.mark.gpu
+
+TOL32 = 1e-4
+TOL64 = 1e-6
+
+
+@pytest.fixture(scope="module")
+def tables_v200804():
+    return synth.lensing("std"), synth.nsx("v200804", seed=0)
+
+
+@pytest.fixture(scope="module")
+def eng_v200804(tables_v200804, golden):
+    lens, nsx = tables_v200804
+    meta, _ = golden
+    e = Engine()
+    e.load_lensing(lens)
+    e.load_nsx(nsx)
+    E, rsp = gc.ism_inst(meta)
+    g = e.add_energy_grid(E)
+    r = e.add_response(g, rsp)
+    e.ism = (g, r, E, rsp)
+    e.g1 = e.add_energy_grid(np.array([1.0]))
+    e.gti = e.add_energy_grid(gc.tinterp_energies())
+    yield e
+    e.close()
+
+
+@pytest.fixture(scope="module")
+def ora_v200804(tables_v200804):
+    return oracle.Oracle(*tables_v200804)
+
+
+def test_devarshi_scenarios(golden, eng_v200804, ora_v200804):
+    meta, z = golden
+    g, r, E, rsp = eng_v200804.ism
+    for s in meta["devarshi"]:
+        p = gc.devarshi_params(s, g, r)
+        for fold in (_abi.FOLD_FP64, _abi.FOLD_FP32, _abi.FOLD_BF16X3):
+            p.fold = fold
+            flux, counts, info = eng_v200804.profile(p)
+            ref_flux, oinfo = ora_v200804.profile(p, E)
+            assert max_rel(flux, ref_flux) < TOL32, (s[0], fold)
+            ref_counts = oracle.fold(rsp, ref_flux, p.exposure_s)
+            assert max_rel(counts, ref_counts) < TOL32, (s[0], fold)
+            assert max_rel(counts, z["devarshi/" + s[0]]) < TOL32, (s[0], fold)
+            assert info.n_active == oinfo.n_active and info.n_points == oinfo.n_points, s[0]
+            assert info.n_dropped_rings == oinfo.n_dropped_rings, s[0]
+
+
+def test_os1_fp64_lightcurves(golden, eng_v200804, ora_v200804):
+    meta, z = golden
+    for s in meta["os1"]:
+        p = gc.os1_params(s, eng_v200804.g1)
+        flux, _, info = eng_v200804.profile(p)
+        ref, oinfo = ora_v200804.profile(p, np.array([1.0]))
+        assert max_rel(flux, ref) < TOL64, s[0]
+        assert max_rel(flux[:, 0], z["os1/" + s[0]]) < TOL64, s[0]
+        assert info.n_points == oinfo.n_points, s[0]
+
+
+def test_all_interpolators(golden, eng_v200804, ora_v200804):
+    meta, z = golden
+    E = gc.tinterp_energies()
+    r0, r1, rs = meta["tinterp_rows"]
+    c0, c1, cs = meta["tinterp_cols"]
+    for s in meta["tinterp"]:
+        p = gc.tinterp_params(s, eng_v200804.gti)
+        flux, _, _ = eng_v200804.profile(p)
+        ref, _ = ora_v200804.profile(p, E)
+        assert max_rel(flux, ref) < TOL32, s[0]
+        assert max_rel(flux[r0:r1:rs, c0:c1:cs], z["tinterp/" + s[0]]) < TOL32, s[0]
+
+
+def test_config1_blackbody_fp64():
+    lens = synth.lensing("std")
+    e = Engine()
+    e.load_lensing(lens)
+    E = synth.energy_grid(64, 0.2, 10.0)
+    g = e.add_energy_grid(E)
+    p = synth.config1_params(g)
+    flux, _, info = e.profile(p)
+    ref, oinfo = oracle.Oracle(lens).profile(p, E)
+    assert info.n_active == oinfo.n_active > 700
+    assert max_rel(flux, ref) < TOL64
+    e.close()
+
+
+@pytest.fixture(scope="module")
+def eng_v171019():
+    lens, nsx = synth.lensing("std"), synth.nsx("v171019", seed=0)
+    e = Engine()
+    e.load_lensing(lens)
+    e.load_nsx(nsx)
+    E = synth.energy_grid(300, 0.2, 12.0)
+    g = e.add_energy_grid(E)
+    rsp = synth.response(300, 1000, E, seed=0)
+    r = e.add_response(g, rsp)
+    e.cfg2 = (g, r, E, rsp)
+    e.ora = oracle.Oracle(lens, nsx)
+    yield e
+    e.close()
+
+
+def test_config2_spots_small_nside(eng_v171019):
+    g, r, E, rsp = eng_v171019.cfg2
+    p = synth.config2_params(g, r, n_side=48, n_bins=16)
+    ref_flux, oinfo = eng_v171019.ora.profile(p, E)
+    ref_counts = oracle.fold(rsp, ref_flux, p.exposure_s)
+    for fold in (_abi.FOLD_FP64, _abi.FOLD_FP32, _abi.FOLD_BF16X3):
+        p.fold = fold
+        flux, counts, info = eng_v171019.profile(p)
+        assert info.n_active == oinfo.n_active and info.n_points == oinfo.n_points
+        assert max_rel(flux, ref_flux) < TOL32
+        assert max_rel(counts, ref_counts) < TOL32, fold
+
+
+def test_batch_matches_plain(eng_v171019):
+    g, r, E, rsp = eng_v171019.cfg2
+    plist, _ = synth.draw_prior(12, seed=3, lens_u=(0.3, 0.5), n_side=32, n_bins=16, energy_grid=g, response=r)
+    flux_b, counts_b, infos = eng_v171019.profile_batch(plist)
+    for k, p in enumerate(plist):
+        f, c, info = eng_v171019.profile(p)
+        assert np.allclose(flux_b[k], f, rtol=1e-12, atol=1e-300), k
+        assert np.allclose(counts_b[k], c, rtol=1e-9, atol=1e-300), k
+        assert infos[k].n_points == info.n_points
+    # and against the oracle for a few
+    for k in range(3):
+        ref, _ = eng_v171019.ora.profile(plist[k], E)
+        assert max_rel(flux_b[k], ref) < TOL32, k
