@@ -1,0 +1,439 @@
+"""Benchmark: batched pulse profiles per second on B200.
+
+Workload (one "step" = one batch): 4096 parameter sets drawn from the batching
+prior (M~U[1,2.2] Msun, R_eq~U[9,15] km, spin~U[100,700] Hz, inclination~U[5,90]
+deg, 1-2 spots of random morphology with angular radius logU[0.01,1] rad,
+logT~U[5.8,6.6]), HEALPix N_side 256, NSX 2l2c_le atmosphere on the synthetic
+v171019-shaped table, 64 phase bins x 2 GL points, 300 log-spaced energies
+0.2-12 keV, 300-channel response fold.  Inputs are seeded synthetic tables of
+the reference's shapes.
+
+  value   batched profiles/s with every input resident in HBM: one CUDA-graph
+          pass (plan -> integrand -> fold) per step, device time by CUDA events
+  e2e     the same through ppm_profile_batch with host parameters in and host
+          counts out (pinned buffers), copies inside the timed region
+  plain   the same kernels launched one profile per call (ppm_profile)
+
+`python bench.py --impl reference` times the FP64 CPU restatement of the
+reference path (oracle/, built with the reference's flags) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "batched profiles/s vs plain at <=1e-4 rel err vs FP64; served p50/p99 latency"
+FLOP_PER_EVAL = 80          # integrand FLOPs per (element, bin, GL node, energy), counted regardless of visibility
+FLOP_PER_FINE = 120         # fine-phase sweep, per integrated ring and fine phase
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-profiles", type=int, default=4096)
+    ap.add_argument("--n-plain", type=int, default=256)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n, seed, synth, abi, g, r):
+    plist, rej = synth.draw_prior(n, seed=seed, lens_u=(0.15, 0.55), n_side=256, n_bins=64, energy_grid=g,
+                                  response=r, fold=abi.FOLD_BF16X3)
+    return plist, rej
+
+
+def n_eval(info, p, n_e):
+    return info.n_active_integrated * p.n_bins * max(p.n_gl, 1) * n_e
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def est_active(p):
+    """Estimated active elements of a profile (spot areas x 12 N_side^2); used only to
+    extrapolate the CPU arm's sampled time to the whole batch."""
+    tot = 0.0
+    pts = _fib_sphere()
+    for s in range(p.n_spots):
+        sp = p.spots[s]
+        if sp.kind == 1:
+            tot += 1
+            continue
+        if sp.angrad2 <= 0:
+            area = 2 * math.pi * (1 - math.cos(sp.angrad1))
+        elif sp.theta1 == sp.theta2 and sp.phi1 == sp.phi2:
+            area = 2 * math.pi * max(0.0, math.cos(sp.angrad2) - math.cos(sp.angrad1))
+        else:
+            def vec(t, f):
+                return np.array([math.sin(t) * math.cos(f), math.sin(t) * math.sin(f), math.cos(t)])
+            inside = (pts @ vec(sp.theta1, sp.phi1) > math.cos(sp.angrad1)) & ~(
+                pts @ vec(sp.theta2, sp.phi2) > math.cos(sp.angrad2))
+            area = 4 * math.pi * inside.mean()
+        tot += area / (4 * math.pi) * 12 * p.n_side * p.n_side
+    return tot
+
+
+_FIB = None
+
+
+def _fib_sphere(m=40000):
+    global _FIB
+    if _FIB is None:
+        k = np.arange(m) + 0.5
+        z = 1 - 2 * k / m
+        phi = math.pi * (3 - math.sqrt(5)) * k
+        r = np.sqrt(1 - z * z)
+        _FIB = np.stack([r * np.cos(phi), r * np.sin(phi), z], 1)
+    return _FIB
+
+
+def run_reference(args):
+    """CPU arm: the FP64 restatement of the reference path on all host cores."""
+    import oracle
+    from gpu_ppm_b200 import _abi, synth
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    lens, nsx = synth.lensing("wide"), synth.nsx("v171019", seed=0)
+    E = synth.energy_grid(300, 0.2, 12.0)
+    plist, _ = synth.draw_prior(args.n_profiles, seed=args.seed, lens_u=(0.15, 0.55), n_side=256, n_bins=64,
+                                energy_grid=0, response=0)
+    ora = oracle.Oracle(lens, nsx, fast=True)
+    cores = os.cpu_count() or 1
+    counts = np.array([est_active(p) for p in plist])
+    evals_full = counts.sum() * 64 * 2 * 300
+    order = np.argsort(counts)
+    times = []
+    samples = []
+    per_step = max(2.0, min(args.cpu_seconds, 12.0))
+    for step in range(args.warmup + args.steps):
+        sample = choose_sample(order, counts, per_step, cores, offset=step)
+        sample = sample[np.argsort(-counts[sample])]  # largest first on the dynamic work queue
+        t0 = time.perf_counter()
+        ora.profile_batch([plist[i] for i in sample], E, n_threads=cores)
+        dt = time.perf_counter() - t0
+        ev = counts[sample].sum() * 64 * 2 * 300
+        if step >= args.warmup:
+            times.append((dt, ev, len(sample)))
+            samples.append(len(sample))
+    rate = sum(e for _, e, _ in times) / sum(t for t, _, _ in times)  # evaluations per second
+    value = args.n_profiles / (evals_full / rate)
+    ms = 1000.0 * sum(t for t, _, _ in times) / len(times)
+    sample_desc = (f"{int(np.mean(samples))} profiles per step spread over the active-element range of the "
+                   f"{args.n_profiles}-profile batch, {cores} threads; profiles/s extrapolated by integrand "
+                   "evaluations (element x bin x GL node x energy, elements estimated from spot areas)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "profiles/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batching prior, N_side 256, NSX 2l2c_le, 64 bins x 2 GL, 300 energies, "
+                               "300-channel fold", "profiles": args.n_profiles},
+        "cpu_baseline": {"value": value, "unit": "profiles/s", "cores": cores, "kind": "port", "sample": sample_desc},
+        "e2e": {"value": value, "unit": "profiles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def choose_sample(order, counts, seconds, cores, offset=0, ns_per_eval=60.0):
+    """Profiles spread over the size distribution whose estimated CPU time fits `seconds`."""
+    budget = seconds * cores * 1e9 / ns_per_eval
+    n = len(order)
+    picked = []
+    tot = 0.0
+    stride = max(1, n // 64)
+    for k in range(offset % stride, n, stride):
+        i = order[k]
+        c = counts[i] * 64 * 2 * 300
+        if tot + c > budget and picked:
+            continue
+        picked.append(i)
+        tot += c
+    return np.array(picked)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+
+    from gpu_ppm_b200 import _abi, synth
+    from gpu_ppm_b200.engine import Engine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    lens, nsx = synth.lensing("wide"), synth.nsx("v171019", seed=0)
+    E = synth.energy_grid(300, 0.2, 12.0)
+    rsp = synth.response(300, 1000, E, seed=0)
+    eng = Engine(device=local)
+    eng.load_lensing(lens)
+    eng.load_nsx(nsx)
+    g = eng.add_energy_grid(E)
+    r = eng.add_response(g, rsp)
+    plist, rejection = workload(args.n_profiles, args.seed + rank, synth, _abi, g, r)
+    n = len(plist)
+
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    batch = eng.batch(plist)
+    flush_buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    # warm-up (also instantiates the graph)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            batch.launch(sh)
+    torch.cuda.synchronize()
+    _, _, infos = batch.collect(want_counts=False)
+    kcount = ctypes.c_int32()
+    _abi.check(_abi.lib().ppm_batch_kernel_count(eng.h, batch.h, ctypes.byref(kcount)))
+
+    # ---- timed region: K graph passes, L2 flushed between passes
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush_buf.zero_()
+                starts[k].record(stream)
+                batch.launch(sh)
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    t_total = sum(step_ms) / 1000.0
+    if dist:
+        t = torch.tensor([t_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_total = float(t.item())
+        dist.barrier()
+    value = world * n * args.steps / t_total
+    ms_per_step = 1000.0 * t_total / args.steps
+
+    # ---- phase times of the same pass (kernel by kernel, events between phases)
+    phases = []
+    ms3 = (ctypes.c_float * 3)()
+    for _ in range(max(2, min(args.steps, 3))):
+        flush_buf.zero_()
+        torch.cuda.synchronize()
+        _abi.check(_abi.lib().ppm_batch_launch_timed(eng.h, batch.h, ctypes.c_void_p(sh), ms3))
+        phases.append(list(ms3))
+    ph = np.mean(np.array(phases), axis=0)
+    integrand_ms = float(ph[1])
+
+    # ---- algorithmic work of one pass
+    evals = sum(n_eval(infos[i], plist[i], len(E)) for i in range(n))
+    rings = sum(max(0, infos[i].n_rings - infos[i].n_dropped_rings) for i in range(n))
+    nf = plist[0].n_fine
+    slice_flops = 2 * 4 * nsx.n[2] * nsx.n[3]
+    alg_flops = FLOP_PER_EVAL * evals + rings * (FLOP_PER_FINE * nf + slice_flops)
+    points = sum(infos[i].n_points for i in range(n))
+    clocks = clk.summary()
+    sm_mhz = clocks["sm_mhz"] or 1965.0
+    props = torch.cuda.get_device_properties(local)
+    fp32_peak = props.multi_processor_count * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the measured clock
+    achieved = alg_flops / (integrand_ms / 1000.0) / 1e12
+    pk, pk_src = peaks()
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "integrand_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tj = json.load(f)
+        if tj.get("evals"):
+            traffic = tj["dram_bytes"] * (evals / tj["evals"])
+
+    # ---- e2e: host parameters in, host counts out, through ppm_profile_batch
+    arr = (_abi.Params * n)(*plist)
+    counts_host = torch.empty(batch.n_counts, dtype=torch.float64, pin_memory=True)
+    cptr = ctypes.cast(ctypes.c_void_p(counts_host.data_ptr()), _abi.DP)
+    infos_e2e = (_abi.ResultInfo * n)()
+    e2e_t = []
+    for k in range(args.warmup + args.steps):
+        flush_buf.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _abi.check(_abi.lib().ppm_profile_batch(eng.h, n, arr, None, cptr, infos_e2e))
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            e2e_t.append(dt)
+    t_e2e = sum(e2e_t)
+    if dist:
+        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e_value = world * n * args.steps / t_e2e
+    h2d = n * ctypes.sizeof(_abi.Params) + 1024 * n  # parameters + converted device profiles (~1 KB each)
+    d2h = batch.n_counts * 8
+
+    # ---- plain form on a prefix of the same profiles
+    n_plain = min(args.n_plain, n)
+    plain_value = plain_equiv = None
+    if n_plain > 0:
+        t0 = time.perf_counter()
+        for i in range(n_plain):
+            eng.profile(plist[i], want_flux=False, want_counts=True)
+        t_plain = time.perf_counter() - t0
+        plain_value = n_plain / t_plain
+        ev_plain = sum(n_eval(infos[i], plist[i], len(E)) for i in range(n_plain))
+        plain_equiv = n / (evals / (ev_plain / t_plain)) if ev_plain else None  # same mix, scaled by evaluations
+
+    # ---- CPU baseline (rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(plist, infos, E, lens, nsx, args)
+
+    batch.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "profiles/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded tables of the reference's shapes)",
+            "config": {
+                "workload": "batching prior: 4096 parameter sets per GPU, N_side 256, NSX 2l2c_le (35x11x166x67), "
+                            "64 bins x 2 GL, 300 energies 0.2-12 keV, 300-channel BF16x3 fold",
+                "profiles_per_step_per_gpu": n, "prior_rejection_rate": round(rejection, 4),
+                "l2": "256 MB buffer written between timed passes; the 629 MB flux pool also exceeds L2",
+                "parallelism": f"replicas x{world}, no collective",
+            },
+            "e2e": {"value": e2e_value, "unit": "profiles/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {
+                "kernel": "integrand_nsx_kernel", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
+                "peak_source": f"FP32 SIMT peak at the measured SM clock: {props.multi_processor_count} SMs x 128 "
+                               f"lanes x 2 x {sm_mhz:.0f} MHz (MEASURED_PEAKS.json {pk_src}: hbm {pk.get('hbm_gbs')} "
+                               f"GB/s, bf16 {pk.get('bf16_tflops')} TF/s)",
+                "flops_per_launch": alg_flops, "integrand_ms": integrand_ms,
+                "convention": "80 FLOP per (element, bin, GL node, energy) regardless of visibility + per integrated "
+                              "ring 120 per fine phase + 2*taps*166*67 slice",
+                "visible_points_per_launch": points, "evaluations_per_launch": evals,
+            },
+            "phases_ms": {"clear_plan": float(ph[0]), "integrand": float(ph[1]), "fold": float(ph[2])},
+            "plain": {"value": plain_value, "unit": "profiles/s", "profiles": n_plain,
+                      "same_mix_extrapolated": plain_equiv,
+                      "batched_over_plain": value / plain_equiv if plain_equiv else None},
+            "gpu_launches": kcount.value * args.steps,
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    eng.close()
+
+
+def cpu_baseline(plist, infos, E, lens, nsx, args):
+    import oracle
+
+    ora = oracle.Oracle(lens, nsx, fast=True)
+    cores = os.cpu_count() or 1
+    ev = np.array([n_eval(infos[i], plist[i], len(E)) for i in range(len(plist))], dtype=np.float64)
+    counts = np.array([infos[i].n_active_integrated for i in range(len(plist))])
+    order = np.argsort(ev)
+    sample = choose_sample(order, counts, args.cpu_seconds, cores)
+    sample = sample[np.argsort(-ev[sample])]  # largest first on the dynamic work queue
+    t0 = time.perf_counter()
+    ora.profile_batch([plist[i] for i in sample], E, n_threads=cores)
+    dt = time.perf_counter() - t0
+    rate = ev[sample].sum() / dt
+    value = len(plist) / (ev.sum() / rate)
+    return {"value": value, "unit": "profiles/s", "cores": cores, "kind": "port",
+            "sample": f"{len(sample)} of the {len(plist)} profiles spread over the size range ({dt:.1f} s on "
+                      f"{cores} threads), extrapolated to the full batch by integrand evaluations"}
+
+
+if __name__ == "__main__":
+    main()

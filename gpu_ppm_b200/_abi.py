@@ -88,7 +88,8 @@ class Params(ctypes.Structure):
 class ResultInfo(ctypes.Structure):
     _fields_ = [
         ("n_active", c_int64), ("n_rings", c_int64), ("n_dropped_rings", c_int64),
-        ("n_points", c_int64), ("n_clamped", c_int64), ("status", c_int32), ("reserved", c_int32),
+        ("n_points", c_int64), ("n_clamped", c_int64), ("n_active_integrated", c_int64),
+        ("status", c_int32), ("reserved", c_int32),
     ]
 
     def as_dict(self):
@@ -115,8 +116,14 @@ SIGNATURES = {
     "ppm_engine_load_ism_inst_dir": (c_int32, [c_void_p, c_char_p, POINTER(c_int32), POINTER(c_int32)]),
     "ppm_profile": (c_int32, [c_void_p, POINTER(Params), DP, DP, POINTER(ResultInfo)]),
     "ppm_profile_batch": (c_int32, [c_void_p, c_int32, POINTER(Params), DP, DP, POINTER(ResultInfo)]),
-    "ppm_profile_batch_device": (c_int32, [c_void_p, c_int32, POINTER(Params), c_void_p, c_void_p, c_void_p,
-                                           c_void_p]),
+    "ppm_batch_create": (c_int32, [c_void_p, c_int32, POINTER(Params), POINTER(c_void_p)]),
+    "ppm_batch_launch": (c_int32, [c_void_p, c_void_p, c_void_p]),
+    "ppm_batch_device_outputs": (c_int32, [c_void_p, POINTER(c_void_p), POINTER(c_int64), POINTER(c_void_p),
+                                           POINTER(c_int64)]),
+    "ppm_batch_collect": (c_int32, [c_void_p, c_void_p, DP, DP, POINTER(ResultInfo)]),
+    "ppm_batch_destroy": (None, [c_void_p, c_void_p]),
+    "ppm_batch_launch_timed": (c_int32, [c_void_p, c_void_p, c_void_p, POINTER(ctypes.c_float)]),
+    "ppm_batch_kernel_count": (c_int32, [c_void_p, c_void_p, POINTER(c_int32)]),
     "ppm_output_sizes": (c_int32, [c_void_p, POINTER(Params), POINTER(c_int64), POINTER(c_int64)]),
     "ppm_submit": (c_int32, [c_void_p, POINTER(Params), DP, DP, POINTER(c_uint64)]),
     "ppm_poll": (c_int32, [c_void_p, c_uint64, POINTER(c_int32)]),

@@ -215,13 +215,64 @@ int ppm_profile_batch(ppm_engine* e, int32_t n, const ppm_params* p, double* flu
   });
 }
 
-int ppm_profile_batch_device(ppm_engine* e, int32_t n, const ppm_params* p_host, const ppm_params* p_device,
-                             double* flux_d, double* counts_d, void* stream) {
+int ppm_batch_create(ppm_engine* e, int32_t n, const ppm_params* p, ppm_batch** out) {
   return guarded([&] {
-    (void)p_device;
-    if (!p_host) throw Error(PPM_E_INVALID, "null params");
-    eng(e).profile_batch_device(n, p_host, flux_d, counts_d, (cudaStream_t)stream);
+    if (!p || !out) throw Error(PPM_E_INVALID, "null params or output handle");
+    *out = nullptr;
+    ppm::BatchImpl* b = new ppm::BatchImpl();
+    try {
+      eng(e).batch_build(*b, n, p);
+    } catch (...) {
+      delete b;
+      throw;
+    }
+    *out = reinterpret_cast<ppm_batch*>(b);
   });
+}
+
+int ppm_batch_launch(ppm_engine* e, ppm_batch* b, void* stream) {
+  return guarded([&] {
+    if (!b) throw Error(PPM_E_INVALID, "null batch");
+    eng(e).batch_launch(*reinterpret_cast<ppm::BatchImpl*>(b), (cudaStream_t)stream);
+  });
+}
+
+int ppm_batch_device_outputs(ppm_batch* b, double** flux, int64_t* n_flux, double** counts, int64_t* n_counts) {
+  return guarded([&] {
+    if (!b) throw Error(PPM_E_INVALID, "null batch");
+    auto* B = reinterpret_cast<ppm::BatchImpl*>(b);
+    if (flux) *flux = B->d_flux;
+    if (n_flux) *n_flux = B->flux_off[B->n];
+    if (counts) *counts = B->d_counts;
+    if (n_counts) *n_counts = B->counts_off[B->n];
+  });
+}
+
+int ppm_batch_collect(ppm_engine* e, ppm_batch* b, double* flux, double* counts, ppm_result_info* info) {
+  return guarded([&] {
+    if (!b) throw Error(PPM_E_INVALID, "null batch");
+    eng(e).batch_collect(*reinterpret_cast<ppm::BatchImpl*>(b), flux, counts, info, nullptr);
+  });
+}
+
+int ppm_batch_launch_timed(ppm_engine* e, ppm_batch* b, void* stream, float* ms) {
+  return guarded([&] {
+    if (!b || !ms) throw Error(PPM_E_INVALID, "null batch or output");
+    eng(e).batch_launch_timed(*reinterpret_cast<ppm::BatchImpl*>(b), (cudaStream_t)stream, ms);
+  });
+}
+
+int ppm_batch_kernel_count(ppm_engine* e, ppm_batch* b, int32_t* n) {
+  return guarded([&] {
+    if (!b || !n) throw Error(PPM_E_INVALID, "null batch or output");
+    *n = eng(e).kernels_per_pass(*reinterpret_cast<ppm::BatchImpl*>(b));
+  });
+}
+
+void ppm_batch_destroy(ppm_engine* e, ppm_batch* b) {
+  if (!b) return;
+  if (e && e->impl) cudaSetDevice(e->impl->cfg.device);
+  delete reinterpret_cast<ppm::BatchImpl*>(b);
 }
 
 int ppm_output_sizes(ppm_engine* e, const ppm_params* p, int64_t* n_flux, int64_t* n_counts) {

@@ -13,7 +13,8 @@
 namespace ppm {
 
 constexpr int kMaxSpots = 2;
-constexpr int kStats = 5;  // n_active, n_rings, n_dropped_rings, n_points, n_clamped
+// per-profile counters: active (integrated rings), rings, dropped rings, points, clamped, active (dropped rings)
+constexpr int kStats = 6;
 
 // ---- resident tables -------------------------------------------------------
 struct DevLens {
@@ -31,6 +32,7 @@ struct DevNsx {
   double inv_dE;       // (nE - 1) / (E_max - E_min): t = (logEkT - E_min) * inv_dE
   const float* data;   // [nT][ng][slice_stride] with slice [nE][nmu], values 10^logInuT3 * 2^scale_exp
   const double* mu;    // [nmu] strictly descending
+  const double* mu_den;  // [nmu - 3][4] reciprocals of the cubic Lagrange denominators per stencil start
   int scale_exp;       // power of two applied to the stored FP32 values
 };
 

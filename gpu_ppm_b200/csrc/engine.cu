@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -58,6 +59,21 @@ void DeviceBuffer::reserve(size_t bytes) {
   if (e != cudaSuccess) throw Error(PPM_E_OOM, std::string("cudaMalloc workspace: ") + cudaGetErrorString(e));
   cap = want;
 }
+void* DeviceArena::alloc(size_t bytes) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) throw Error(PPM_E_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  ptrs.push_back(p);
+  bytes_held += bytes;
+  return p;
+}
+DeviceArena::~DeviceArena() {
+  for (void* p : ptrs) cudaFree(p);
+}
+BatchImpl::~BatchImpl() {
+  if (graph) cudaGraphExecDestroy(graph);
+}
+
 void DeviceBuffer::release() {
   if (ptr) cudaFree(ptr);
   ptr = nullptr;
@@ -88,7 +104,12 @@ Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   PPM_CUDA(cudaSetDevice(cfg.device));
   PPM_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, cfg.device));
   PPM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-  for (int k = 0; k < 3; ++k) PPM_CUDA(cudaEventCreate(&ev[k]));
+  // launch-shape overrides for experiments: PPM_PB, PPM_CHUNK, PPM_NE_T, PPM_MINB
+  if (const char* v = std::getenv("PPM_PB")) tune.pb = std::max(1, std::atoi(v));
+  if (const char* v = std::getenv("PPM_CHUNK")) tune.chunk = std::max(32, std::atoi(v));
+  if (const char* v = std::getenv("PPM_NE_T")) tune.ne_t = std::atoi(v);
+  if (const char* v = std::getenv("PPM_MINB")) tune.minb = std::max(1, std::min(2, std::atoi(v)));
+  for (int k = 0; k < 4; ++k) PPM_CUDA(cudaEventCreate(&ev[k]));
 }
 
 Engine::~Engine() {
@@ -98,17 +119,7 @@ Engine::~Engine() {
   for (void* p : owned) cudaFree(p);
   for (auto& kv : ring_tabs) cudaFree(kv.second);
   for (auto& kv : fine_tabs) cudaFree(kv.second);
-  ws_prof.release();
-  ws_flux.release();
-  ws_counts.release();
-  ws_stats.release();
-  ws_tiles.release();
-  ws_ctrl.release();
-  ws_jobs.release();
-  h_stage.release();
-  h_out.release();
-  for (auto& g : graphs) cudaGraphExecDestroy(g.second.exec);
-  for (int k = 0; k < 3; ++k) cudaEventDestroy(ev[k]);
+  for (int k = 0; k < 4; ++k) cudaEventDestroy(ev[k]);
   cudaStreamDestroy(stream);
 }
 
@@ -172,8 +183,19 @@ void Engine::load_nsx(const ppm_nsx_desc& d) {
     for (size_t k = 0; k < slice; ++k) h[sl * stride + k] = (float)std::ldexp(lin[sl * slice + k], scale_exp);
   float* data = dev_upload(h.data(), h.size());
   double* mu = dev_upload(d.mu, (size_t)d.n_mu);
+  // 1 / ((x_j - x_k)(x_j - x_l)(x_j - x_m)) of each 4-node mu stencil (cpu/nsx.hpp:159-168)
+  std::vector<double> den(4 * (size_t)(d.n_mu - 3));
+  for (int st = 0; st + 3 < d.n_mu; ++st) {
+    const double* x = d.mu + st;
+    den[4 * st + 0] = 1.0 / ((x[0] - x[1]) * (x[0] - x[2]) * (x[0] - x[3]));
+    den[4 * st + 1] = 1.0 / ((x[1] - x[0]) * (x[1] - x[2]) * (x[1] - x[3]));
+    den[4 * st + 2] = 1.0 / ((x[2] - x[0]) * (x[2] - x[1]) * (x[2] - x[3]));
+    den[4 * st + 3] = 1.0 / ((x[3] - x[0]) * (x[3] - x[1]) * (x[3] - x[2]));
+  }
+  double* mu_den = dev_upload(den.data(), den.size());
   track(data);
   track(mu);
+  track(mu_den);
   DevNsx X{};
   X.nT = d.n_logT;
   X.ng = d.n_logg;
@@ -189,6 +211,7 @@ void Engine::load_nsx(const ppm_nsx_desc& d) {
   X.inv_dE = (d.n_logEkT - 1) / (d.logEkT_max - d.logEkT_min);
   X.data = data;
   X.mu = mu;
+  X.mu_den = mu_den;
   X.scale_exp = scale_exp;
   nsx = X;
   nsx_mu.assign(d.mu, d.mu + d.n_mu);
@@ -493,27 +516,15 @@ void Engine::to_device(const ppm_params& p, DevProfile& d, long long flux_off, u
   }
 }
 
-// ---- workspace and launches ----------------------------------------------------------
-long long Engine::tile_bound(const ppm_params& p, int chunk) {
-  long long b = 0;
-  const int N = p.n_side;
-  const std::vector<double>& rt = host_rings[N];
-  (void)rt;
-  for (int s = 0; s < p.n_spots; ++s) {
-    if (p.spots[s].kind == PPM_SPOT_POINT) {
-      b += 1;
-      continue;
-    }
-    // rings in range x (two ranges + chunks per range)
-    long long rings = 4ll * N - 1;
-    long long per = 2 + (4ll * N + chunk - 1) / chunk;
-    b += rings * per;
-  }
-  return b;
-}
-
-void Engine::run(int n, const ppm_params* ps, double* ext_flux, double* ext_counts, Batch& B, cudaStream_t st) {
+// ---- batches ----------------------------------------------------------------------
+// Converts and uploads n profiles, sizes the work queue and output pools, and
+// records the launch shapes; the batch owns all of its device memory.
+void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps) {
+  if (n < 1) throw Error(PPM_E_INVALID, "empty batch");
+  if (n > cfg.max_batch) throw Error(PPM_E_RANGE, "batch larger than max_batch");
+  PPM_CUDA(cudaSetDevice(cfg.device));
   B.n = n;
+  B.params.assign(ps, ps + n);
   B.flux_off.assign(n + 1, 0);
   B.counts_off.assign(n + 1, 0);
   for (int i = 0; i < n; ++i) {
@@ -524,86 +535,78 @@ void Engine::run(int n, const ppm_params* ps, double* ext_flux, double* ext_coun
     const long long nc = ps[i].response >= 0 ? (long long)resps[ps[i].response].n_ch * ps[i].n_bins : 0;
     B.counts_off[i + 1] = B.counts_off[i] + nc;
   }
-  // groups by kernel variant: 0 = NSX, 1 = blackbody FP64, 2 = blackbody FP32
+  // kernel variants: 0 = NSX, 1 = blackbody FP64, 2 = blackbody FP32
+  auto variant = [](const ppm_params& p) {
+    return p.atmosphere == PPM_ATM_NSX ? 0 : (p.precision == PPM_PREC_FP64 ? 1 : 2);
+  };
   std::vector<int> order;
   order.reserve(n);
   for (int v = 0; v < 3; ++v)
-    for (int i = 0; i < n; ++i) {
-      int var = ps[i].atmosphere == PPM_ATM_NSX ? 0 : (ps[i].precision == PPM_PREC_FP64 ? 1 : 2);
-      if (var == v) order.push_back(i);
-    }
+    for (int i = 0; i < n; ++i)
+      if (variant(ps[i]) == v) order.push_back(i);
   const int chunk = tune.chunk;
-  // device profiles in group order
+  B.d_stats = (unsigned long long*)B.mem.alloc(sizeof(unsigned long long) * kStats * (size_t)n);
   std::vector<DevProfile> hp(n);
-  ws_stats.reserve(sizeof(unsigned long long) * kStats * (size_t)n);
-  unsigned long long* d_stats = (unsigned long long*)ws_stats.ptr;
-  long long tiles_total = 0;
-  std::vector<long long> tiles_group(3, 0);
-  std::vector<int> group_start(4, 0);
+  long long cap[3] = {0, 0, 0};
+  int start[4] = {0, 0, 0, 0};
   for (int k = 0; k < n; ++k) {
     const int i = order[k];
-    to_device(ps[i], hp[k], B.flux_off[i], d_stats + (size_t)kStats * i);
-    int var = ps[i].atmosphere == PPM_ATM_NSX ? 0 : (ps[i].precision == PPM_PREC_FP64 ? 1 : 2);
-    tiles_group[var] += tile_bound(ps[i], chunk);
-    group_start[var + 1] = k + 1;
+    to_device(ps[i], hp[k], B.flux_off[i], B.d_stats + (size_t)kStats * i);
+    const int v = variant(ps[i]);
+    for (int s = 0; s < ps[i].n_spots; ++s) {
+      const DevSpot& sp = hp[k].spot[s];
+      if (sp.kind == PPM_SPOT_POINT) {
+        cap[v] += 1;
+      } else if (sp.i_hi >= sp.i_lo) {
+        const long long rings = sp.i_hi - sp.i_lo + 1;
+        cap[v] += rings * (2 + (4ll * ps[i].n_side + chunk - 1) / chunk);
+      }
+    }
+    start[v + 1] = k + 1;
   }
-  for (int v = 1; v <= 3; ++v) group_start[v] = std::max(group_start[v], group_start[v - 1]);
-  for (int v = 0; v < 3; ++v) tiles_total += tiles_group[v];
-  if (tiles_total > (1ll << 31) - 1) throw Error(PPM_E_RANGE, "batch too large for one work queue");
-
-  ws_prof.reserve(sizeof(DevProfile) * (size_t)n);
-  ws_flux.reserve(sizeof(double) * (size_t)std::max(1ll, B.flux_off[n]));
-  ws_counts.reserve(sizeof(double) * (size_t)std::max(1ll, B.counts_off[n]));
-  ws_tiles.reserve(sizeof(Tile) * (size_t)std::max(1ll, tiles_total));
-  ws_ctrl.reserve(sizeof(int) * 16);
-  // the pinned staging buffer may still feed the previous batch's copy
-  PPM_CUDA(cudaEventSynchronize(ev[0]));
-  h_stage.reserve(sizeof(DevProfile) * (size_t)n);
-  std::memcpy(h_stage.ptr, hp.data(), sizeof(DevProfile) * (size_t)n);
-  DevProfile* d_prof = (DevProfile*)ws_prof.ptr;
-  B.d_flux = ext_flux ? ext_flux : (double*)ws_flux.ptr;
-  B.d_counts = ext_counts ? ext_counts : (double*)ws_counts.ptr;
-  B.d_stats = d_stats;
-
-  PPM_CUDA(cudaMemcpyAsync(d_prof, h_stage.ptr, sizeof(DevProfile) * (size_t)n, cudaMemcpyHostToDevice, st));
-  PPM_CUDA(cudaEventRecord(ev[0], st));
-  PPM_CUDA(cudaMemsetAsync(B.d_flux, 0, sizeof(double) * (size_t)B.flux_off[n], st));
-  PPM_CUDA(cudaMemsetAsync(d_stats, 0, sizeof(unsigned long long) * kStats * (size_t)n, st));
-  PPM_CUDA(cudaMemsetAsync(ws_ctrl.ptr, 0, sizeof(int) * 16, st));
-  int* ctrl = (int*)ws_ctrl.ptr;
-
-  long long tile_base = 0;
+  for (int v = 1; v <= 3; ++v) start[v] = std::max(start[v], start[v - 1]);
+  const long long cap_total = cap[0] + cap[1] + cap[2];
+  if (cap_total > (1ll << 31) - 1) throw Error(PPM_E_RANGE, "batch too large for one work queue");
+  B.d_prof = (DevProfile*)B.mem.alloc(sizeof(DevProfile) * (size_t)n);
+  B.d_flux = (double*)B.mem.alloc(sizeof(double) * (size_t)std::max(1ll, B.flux_off[n]));
+  B.d_counts = (double*)B.mem.alloc(sizeof(double) * (size_t)std::max(1ll, B.counts_off[n]));
+  Tile* tiles = (Tile*)B.mem.alloc(sizeof(Tile) * (size_t)std::max(1ll, cap_total));
+  B.d_ctrl = (int*)B.mem.alloc(sizeof(int) * 16);
+  PPM_CUDA(cudaMemcpy(B.d_prof, hp.data(), sizeof(DevProfile) * (size_t)n, cudaMemcpyHostToDevice));
+  B.h2d_bytes = sizeof(DevProfile) * (size_t)n;
+  long long base = 0;
+  B.groups.clear();
   for (int v = 0; v < 3; ++v) {
-    const int g0 = group_start[v], g1 = group_start[v + 1];
+    const int g0 = start[v], g1 = start[v + 1];
     if (g1 <= g0) continue;
-    WorkQueue q{};
-    q.tiles = (Tile*)ws_tiles.ptr + tile_base;
-    q.capacity = (int)tiles_group[v];
-    q.n_tiles = ctrl + 3 * v;
-    q.next = ctrl + 3 * v + 1;
-    q.overflow = ctrl + 3 * v + 2;
-    tile_base += tiles_group[v];
-    PPM_CUDA(launch_plan(d_prof + g0, g1 - g0, lens, q, chunk, st));
-    // launch shape
-    int ne_max = 1, nf_max = 2, cells_max = 1;
+    BatchImpl::Group G;
+    G.g0 = g0;
+    G.g1 = g1;
+    WorkQueue& q = G.args.queue;
+    q.tiles = tiles + base;
+    q.capacity = (int)cap[v];
+    q.n_tiles = B.d_ctrl + 3 * v;
+    q.next = B.d_ctrl + 3 * v + 1;
+    q.overflow = B.d_ctrl + 3 * v + 2;
+    base += cap[v];
+    int ne_max = 1, nf_max = 2, cells_max = 2;
     for (int k = g0; k < g1; ++k) {
       ne_max = std::max(ne_max, hp[k].n_e);
       nf_max = std::max(nf_max, hp[k].n_fine);
       cells_max = std::max(cells_max, hp[k].grid.span + 1);
     }
-    KernelArgs a{};
-    a.profiles = d_prof + g0;
-    a.lens = lens;
-    a.nsx = nsx;
-    a.queue = q;
-    a.flux = B.d_flux;
-    a.shape = choose_shape(v == 0, v == 1, ne_max, nf_max, cells_max);
-    PPM_CUDA(configure_integrand_smem(a.shape));
-    int occ = max_active_ctas(a.shape);
-    if (occ < 1) throw Error(PPM_E_RANGE, "integrand launch shape does not fit on an SM (shared memory " +
-                                              std::to_string(a.shape.total) + " bytes)");
-    long long grid = std::min<long long>((long long)sm_count * occ, tiles_group[v]);
-    PPM_CUDA(launch_integrand(a, (int)grid, st));
+    G.args.profiles = B.d_prof + g0;
+    G.args.lens = lens;
+    G.args.nsx = nsx;
+    G.args.flux = B.d_flux;
+    G.args.shape = choose_shape(v == 0, v == 1, ne_max, nf_max, cells_max);
+    PPM_CUDA(configure_integrand_smem(G.args.shape));
+    const int occ = max_active_ctas(G.args.shape);
+    if (occ < 1)
+      throw Error(PPM_E_RANGE, "integrand launch shape does not fit on an SM (" + std::to_string(G.args.shape.total) +
+                                   " bytes of shared memory)");
+    G.grid = (int)std::min<long long>((long long)sm_count * occ, std::max(1ll, cap[v]));
+    B.groups.push_back(G);
   }
   // folds grouped by (response, n_bins, arithmetic)
   std::map<std::tuple<int, int, int>, std::vector<FoldJob>> folds;
@@ -612,29 +615,137 @@ void Engine::run(int n, const ppm_params* ps, double* ext_flux, double* ext_coun
     FoldJob j{B.flux_off[i], B.counts_off[i], ps[i].exposure_s * (1. / ps[i].n_bins)};
     folds[std::make_tuple(ps[i].response, ps[i].n_bins, ps[i].fold)].push_back(j);
   }
-  size_t njobs = 0;
-  for (auto& kv : folds) njobs += kv.second.size();
-  if (njobs) {
-    ws_jobs.reserve(sizeof(FoldJob) * njobs);
-    h_jobs.resize(njobs);
-    size_t k = 0;
-    for (auto& kv : folds)
-      for (auto& j : kv.second) h_jobs[k++] = j;
-    PPM_CUDA(cudaMemcpyAsync(ws_jobs.ptr, h_jobs.data(), sizeof(FoldJob) * njobs, cudaMemcpyHostToDevice, st));
-    k = 0;
-    for (auto& kv : folds) {
-      const Resp& r = resps[std::get<0>(kv.first)];
-      const int nb = std::get<1>(kv.first), mode = std::get<2>(kv.first);
-      const FoldJob* jobs = (const FoldJob*)ws_jobs.ptr + k;
-      const int nj = (int)kv.second.size();
-      if (mode == PPM_FOLD_BF16X3 && r.tc_ok)
-        PPM_CUDA(fold_tc_launch(r, jobs, nj, nb, B.d_flux, B.d_counts, st));
-      else
-        PPM_CUDA(launch_fold_simt(jobs, nj, r.d_rsp, r.n_ch, r.n_e, nb, B.d_flux, B.d_counts,
-                                  mode != PPM_FOLD_FP32, st));
-      k += nj;
+  std::vector<FoldJob> jobs;
+  B.folds.clear();
+  for (auto& kv : folds) {
+    BatchImpl::Fold f{std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first), (int)jobs.size(),
+                      (int)kv.second.size()};
+    B.folds.push_back(f);
+    jobs.insert(jobs.end(), kv.second.begin(), kv.second.end());
+  }
+  if (!jobs.empty()) {
+    B.d_jobs = (FoldJob*)B.mem.alloc(sizeof(FoldJob) * jobs.size());
+    PPM_CUDA(cudaMemcpy(B.d_jobs, jobs.data(), sizeof(FoldJob) * jobs.size(), cudaMemcpyHostToDevice));
+    B.h2d_bytes += sizeof(FoldJob) * jobs.size();
+  }
+}
+
+// One pass: clear outputs and queue, plan, integrate, fold.  With `events`,
+// records events[0..3] around the phases.
+void Engine::batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events) {
+  const int n = B.n;
+  if (events) PPM_CUDA(cudaEventRecord(events[0], st));
+  PPM_CUDA(cudaMemsetAsync(B.d_flux, 0, sizeof(double) * (size_t)B.flux_off[n], st));
+  PPM_CUDA(cudaMemsetAsync(B.d_stats, 0, sizeof(unsigned long long) * kStats * (size_t)n, st));
+  PPM_CUDA(cudaMemsetAsync(B.d_ctrl, 0, sizeof(int) * 16, st));
+  for (const auto& G : B.groups) PPM_CUDA(launch_plan(B.d_prof + G.g0, G.g1 - G.g0, lens, G.args.queue, tune.chunk, st));
+  if (events) PPM_CUDA(cudaEventRecord(events[1], st));
+  for (const auto& G : B.groups) PPM_CUDA(launch_integrand(G.args, G.grid, st));
+  if (events) PPM_CUDA(cudaEventRecord(events[2], st));
+  for (const auto& f : B.folds) {
+    const Resp& r = resps[f.resp];
+    const FoldJob* jobs = B.d_jobs + f.job0;
+    if (f.mode == PPM_FOLD_BF16X3 && r.tc_ok)
+      PPM_CUDA(fold_tc_launch(r, jobs, f.n_jobs, f.n_bins, B.d_flux, B.d_counts, st));
+    else
+      PPM_CUDA(launch_fold_simt(jobs, f.n_jobs, r.d_rsp, r.n_ch, r.n_e, f.n_bins, B.d_flux, B.d_counts,
+                                f.mode != PPM_FOLD_FP32, st));
+  }
+  if (events) PPM_CUDA(cudaEventRecord(events[3], st));
+}
+
+void Engine::batch_launch_timed(BatchImpl& B, cudaStream_t st, float* ms) {
+  std::lock_guard<std::mutex> lk(mu);
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  if (!st) st = stream;
+  batch_enqueue(B, st, ev);
+  B.last_stream = st;
+  PPM_CUDA(cudaEventSynchronize(ev[3]));
+  for (int k = 0; k < 3; ++k) PPM_CUDA(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
+}
+
+int Engine::kernels_per_pass(const BatchImpl& B) const { return 2 * (int)B.groups.size() + (int)B.folds.size(); }
+
+void Engine::batch_capture(BatchImpl& B) {
+  cudaStream_t cs;
+  PPM_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    try {
+      batch_enqueue(B, cs, nullptr);
+    } catch (...) {
+      cudaStreamEndCapture(cs, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaStreamDestroy(cs);
+      throw;
+    }
+    e = cudaStreamEndCapture(cs, &g);
+  }
+  cudaStreamDestroy(cs);
+  if (e != cudaSuccess) throw Error(PPM_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&B.graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) throw Error(PPM_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+}
+
+void Engine::batch_launch(BatchImpl& B, cudaStream_t st) {
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  if (!st) st = stream;
+  if (!B.graph) batch_capture(B);
+  PPM_CUDA(cudaGraphLaunch(B.graph, st));
+  B.last_stream = st;
+}
+
+void Engine::batch_collect(BatchImpl& B, double* flux, double* counts, ppm_result_info* info, cudaStream_t st) {
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  if (!st) st = B.last_stream ? B.last_stream : stream;
+  const int n = B.n;
+  std::vector<unsigned long long> stats((size_t)kStats * n);
+  int ctrl[16];
+  if (flux)
+    PPM_CUDA(cudaMemcpyAsync(flux, B.d_flux, sizeof(double) * (size_t)B.flux_off[n], cudaMemcpyDeviceToHost, st));
+  if (counts && B.counts_off[n] > 0)
+    PPM_CUDA(cudaMemcpyAsync(counts, B.d_counts, sizeof(double) * (size_t)B.counts_off[n], cudaMemcpyDeviceToHost, st));
+  PPM_CUDA(cudaMemcpyAsync(stats.data(), B.d_stats, sizeof(unsigned long long) * stats.size(), cudaMemcpyDeviceToHost,
+                           st));
+  PPM_CUDA(cudaMemcpyAsync(ctrl, B.d_ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, st));
+  PPM_CUDA(cudaStreamSynchronize(st));
+  PPM_CUDA(cudaGetLastError());
+  if (ctrl[2] || ctrl[5] || ctrl[8]) throw Error(PPM_E_RANGE, "work queue overflow");
+  if (info) {
+    for (int i = 0; i < n; ++i) {
+      ppm_result_info& r = info[i];
+      const unsigned long long* s = &stats[(size_t)kStats * i];
+      r.n_active = (int64_t)(s[0] + s[5]);
+      r.n_rings = (int64_t)s[1];
+      r.n_dropped_rings = (int64_t)s[2];
+      r.n_points = (int64_t)s[3];
+      r.n_clamped = (int64_t)s[4];
+      r.n_active_integrated = (int64_t)s[0];
+      r.status = PPM_OK;
+      r.reserved = 0;
     }
   }
+}
+
+void Engine::profile(const ppm_params& p, double* flux, double* counts, ppm_result_info* info) {
+  std::lock_guard<std::mutex> lk(mu);
+  if (counts && p.response < 0) throw Error(PPM_E_INVALID, "counts requested without a response");
+  BatchImpl B;
+  batch_build(B, 1, &p);
+  batch_enqueue(B, stream, nullptr);  // plain form: direct launches, no graph
+  B.last_stream = stream;
+  batch_collect(B, flux, counts, info, stream);
+}
+
+void Engine::profile_batch(int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info) {
+  std::lock_guard<std::mutex> lk(mu);
+  BatchImpl B;
+  batch_build(B, n, ps);
+  batch_enqueue(B, stream, nullptr);
+  B.last_stream = stream;
+  batch_collect(B, flux, counts, info, stream);
 }
 
 IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max) {
@@ -647,75 +758,18 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
   int nt = (ne_max + ne_t - 1) / ne_t;
   nt = (nt + 31) / 32 * 32;
   nt = std::max(64, std::min(512, nt));
-  int pb = std::min(tune.pb, nt);
+  // whole multiples of the warp count keep the one-warp-per-point build balanced
+  const int nwarps = nt / 32;
+  int pb = std::max(nwarps, (std::min(tune.pb, nt) / nwarps) * nwarps);
   IntegrandShape s;
   for (;;) {
     s = make_shape(nsx_kernel, nt, ne_t, pb, tune.chunk, nf_max, lens.n_cp, lens.n_ca, nsx.nE, nsx.nmu, cells_max);
-    if (s.total <= 200 * 1024 || pb <= 4) break;
-    pb /= 2;
+    if (s.total <= 200 * 1024 || pb <= nwarps) break;
+    pb -= nwarps;
   }
   s.bb_fp64 = bb_fp64 ? 1 : 0;
+  s.minb = (ne_t <= 2 && nt <= 320) ? tune.minb : 1;
   return s;
-}
-
-void Engine::collect(const Batch& B, int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info,
-                     cudaStream_t st) {
-  if (flux) {
-    h_out.reserve(sizeof(double) * (size_t)B.flux_off[n]);
-    PPM_CUDA(cudaMemcpyAsync(h_out.ptr, B.d_flux, sizeof(double) * (size_t)B.flux_off[n], cudaMemcpyDeviceToHost, st));
-  }
-  std::vector<unsigned long long> stats((size_t)kStats * n);
-  PPM_CUDA(cudaMemcpyAsync(stats.data(), B.d_stats, sizeof(unsigned long long) * stats.size(), cudaMemcpyDeviceToHost,
-                           st));
-  int ctrl[16];
-  PPM_CUDA(cudaMemcpyAsync(ctrl, ws_ctrl.ptr, sizeof(ctrl), cudaMemcpyDeviceToHost, st));
-  PPM_CUDA(cudaStreamSynchronize(st));
-  if (ctrl[2] || ctrl[5] || ctrl[8]) throw Error(PPM_E_RANGE, "work queue overflow");
-  if (flux) std::memcpy(flux, h_out.ptr, sizeof(double) * (size_t)B.flux_off[n]);
-  if (counts && B.counts_off[n] > 0) {
-    PPM_CUDA(cudaMemcpy(counts, B.d_counts, sizeof(double) * (size_t)B.counts_off[n], cudaMemcpyDeviceToHost));
-  }
-  if (info) {
-    for (int i = 0; i < n; ++i) {
-      ppm_result_info& r = info[i];
-      r.n_active = (int64_t)stats[kStats * i + 0];
-      r.n_rings = (int64_t)stats[kStats * i + 1];
-      r.n_dropped_rings = (int64_t)stats[kStats * i + 2];
-      r.n_points = (int64_t)stats[kStats * i + 3];
-      r.n_clamped = (int64_t)stats[kStats * i + 4];
-      r.status = PPM_OK;
-      r.reserved = 0;
-    }
-  }
-}
-
-void Engine::profile(const ppm_params& p, double* flux, double* counts, ppm_result_info* info) {
-  std::lock_guard<std::mutex> lk(mu);
-  PPM_CUDA(cudaSetDevice(cfg.device));
-  if (counts && p.response < 0) throw Error(PPM_E_INVALID, "counts requested without a response");
-  Batch B;
-  run(1, &p, nullptr, nullptr, B, stream);
-  collect(B, 1, &p, flux, counts, info, stream);
-}
-
-void Engine::profile_batch(int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info) {
-  if (n < 1) throw Error(PPM_E_INVALID, "empty batch");
-  if (n > cfg.max_batch) throw Error(PPM_E_RANGE, "batch larger than max_batch");
-  std::lock_guard<std::mutex> lk(mu);
-  PPM_CUDA(cudaSetDevice(cfg.device));
-  Batch B;
-  run(n, ps, nullptr, nullptr, B, stream);
-  collect(B, n, ps, flux, counts, info, stream);
-}
-
-// Device-resident form: outputs land in caller device buffers, nothing is synchronised.
-void Engine::profile_batch_device(int n, const ppm_params* ps, double* flux_d, double* counts_d, cudaStream_t st) {
-  if (n < 1) throw Error(PPM_E_INVALID, "empty batch");
-  if (!flux_d) throw Error(PPM_E_INVALID, "flux_device is required");
-  std::lock_guard<std::mutex> lk(mu);
-  PPM_CUDA(cudaSetDevice(cfg.device));
-  Batch B;
-  run(n, ps, flux_d, counts_d, B, st ? st : stream);
 }
 
 void Engine::output_sizes(const ppm_params& p, int64_t* n_flux, int64_t* n_counts) const {

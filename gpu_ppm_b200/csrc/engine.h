@@ -61,18 +61,52 @@ struct Resp {
   void* d_a_lo = nullptr;
 };
 
-struct Batch {
+// Device allocations owned by one batch.
+struct DeviceArena {
+  std::vector<void*> ptrs;
+  size_t bytes_held = 0;
+  void* alloc(size_t bytes);
+  DeviceArena() = default;
+  DeviceArena(const DeviceArena&) = delete;
+  DeviceArena& operator=(const DeviceArena&) = delete;
+  ~DeviceArena();
+};
+
+// A converted, uploaded and planned set of profiles with its output pools.
+struct BatchImpl {
   int n = 0;
+  std::vector<ppm_params> params;
   std::vector<long long> flux_off, counts_off;
+  DeviceArena mem;
+  DevProfile* d_prof = nullptr;
   double* d_flux = nullptr;
   double* d_counts = nullptr;
   unsigned long long* d_stats = nullptr;
+  int* d_ctrl = nullptr;
+  FoldJob* d_jobs = nullptr;
+  struct Group {
+    int g0 = 0, g1 = 0, grid = 0;
+    KernelArgs args{};
+  };
+  struct Fold {
+    int resp, n_bins, mode, job0, n_jobs;
+  };
+  std::vector<Group> groups;
+  std::vector<Fold> folds;
+  size_t h2d_bytes = 0;
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t last_stream = nullptr;
+  BatchImpl() = default;
+  BatchImpl(const BatchImpl&) = delete;
+  BatchImpl& operator=(const BatchImpl&) = delete;
+  ~BatchImpl();
 };
 
 struct Tuning {
-  int pb = 32;       // phase points per batch
+  int pb = 20;       // phase points per polynomial sub-batch (rounded to whole warps)
   int chunk = 1024;  // candidate elements per tile
   int ne_t = 0;      // energies per thread (0 = automatic)
+  int minb = 2;      // CTAs per SM targeted by the register budget
 };
 
 struct GraphEntry {
@@ -93,7 +127,13 @@ class Engine {
 
   void profile(const ppm_params& p, double* flux, double* counts, ppm_result_info* info);
   void profile_batch(int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info);
-  void profile_batch_device(int n, const ppm_params* ps_host, double* flux_d, double* counts_d, cudaStream_t st);
+  void batch_build(BatchImpl& B, int n, const ppm_params* ps);
+  void batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events);
+  void batch_capture(BatchImpl& B);
+  void batch_launch(BatchImpl& B, cudaStream_t st);
+  void batch_collect(BatchImpl& B, double* flux, double* counts, ppm_result_info* info, cudaStream_t st);
+  int kernels_per_pass(const BatchImpl& B) const;
+  void batch_launch_timed(BatchImpl& B, cudaStream_t st, float* ms);
   void output_sizes(const ppm_params& p, int64_t* n_flux, int64_t* n_counts) const;
 
   // serving
@@ -116,11 +156,7 @@ class Engine {
   DevGrid dev_grid(int id);
   const double* ring_table(int N);
   const double* fine_table(int nf);
-  long long tile_bound(const ppm_params& p, int chunk);
   IntegrandShape choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max);
-  void run(int n, const ppm_params* ps, double* ext_flux, double* ext_counts, Batch& B, cudaStream_t st);
-  void collect(const Batch& B, int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info,
-               cudaStream_t st);
   void fold_tc_prepare(Resp& r);
   cudaError_t fold_tc_launch(const Resp& r, const FoldJob* jobs, int n_jobs, int n_bins, const double* flux,
                              double* counts, cudaStream_t st);
@@ -137,11 +173,7 @@ class Engine {
   std::map<int, double*> ring_tabs, fine_tabs;
   std::map<int, std::vector<double>> host_rings;
   std::vector<void*> owned;
-  DeviceBuffer ws_prof, ws_flux, ws_counts, ws_stats, ws_tiles, ws_ctrl, ws_jobs;
-  HostBuffer h_stage, h_out;
-  std::vector<FoldJob> h_jobs;
-  std::map<std::string, GraphEntry> graphs;
-  cudaEvent_t ev[3];
+  cudaEvent_t ev[4];
 
   // serving state
   struct Server* server = nullptr;

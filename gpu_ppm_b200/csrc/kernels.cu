@@ -215,8 +215,8 @@ __device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtr
 }
 
 // ---------------------------------------------------------------------------
-template <int NE_T>
-__global__ void __launch_bounds__(512) integrand_nsx_kernel(const KernelArgs a) {
+template <int NE_T, int MINB>
+__global__ void __launch_bounds__(MINB == 1 ? 512 : 320, MINB) integrand_nsx_kernel(const KernelArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
   const IntegrandShape& S = a.shape;
   const SmemPtrs s = carve(sm, S);
@@ -230,13 +230,11 @@ __global__ void __launch_bounds__(512) integrand_nsx_kernel(const KernelArgs a) 
   const DevNsx& X = a.nsx;
   const int nE = X.nE, nmu = X.nmu, cells = S.cells, HN = cells + 3;
 
-  // batch SoA
-  float* b_c = (float*)s.batch;
-  float* b_fP = b_c + S.pb;
-  int* b_G0 = (int*)(b_fP + S.pb);
-  int* b_bin = b_G0 + S.pb;
-  int* b_imu = b_bin + S.pb;
-  float* b_w = (float*)(b_imu + S.pb);  // [4][pb]
+  // point records, one slot per thread: {c, fP, bin, G0} packed for one broadcast load,
+  // plus the mu stencil start and weights
+  float4* r_pk = (float4*)s.batch;
+  int* r_imu = (int*)(r_pk + nt);
+  float* r_w = (float*)(r_imu + nt);  // [4][nt]
 
   for (;;) {
     __syncthreads();
@@ -281,6 +279,7 @@ __global__ void __launch_bounds__(512) integrand_nsx_kernel(const KernelArgs a) 
       s_ntap = n;
     }
     for (int k = tid; k < nmu; k += nt) s.mu[k] = X.mu[k];
+    for (int k = tid; k < 4 * (nmu - 3); k += nt) s.mu[nmu + k] = X.mu_den[k];
     __syncthreads();
     {
       const int n4 = X.slice_stride >> 2, ntap = s_ntap;
@@ -334,14 +333,17 @@ __global__ void __launch_bounds__(512) integrand_nsx_kernel(const KernelArgs a) 
       }
     };
 
-    for (int q0 = 0; q0 < n_pts; q0 += S.pb) {
-      // stage A: phase points -> batch (visible ones, order kept)
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nt >> 5;
+    const double* den = s.mu + nmu;  // [nmu - 3][4] reciprocal Lagrange denominators
+    for (int q0 = 0; q0 < n_pts; q0 += nt) {
+      // stage A: every thread evaluates one phase point (FP64); visible ones are
+      // compacted, in order, into the point records
       bool vis = false, clamped = false;
       float c = 0.f, fP = 0.f;
       int G0 = 0, bin = 0, imu = 0;
       float w4[4] = {0.f, 0.f, 0.f, 0.f};
       const int q = q0 + tid;
-      if (tid < S.pb && q < n_pts) {
+      if (q < n_pts) {
         double wgl, z = 0, mu = 0;
         const double flux = phase_point(p, s, tile.ring, point, n_act, q, bin, wgl, z, mu);
         if (flux != 0.0) {
@@ -351,119 +353,145 @@ __global__ void __launch_bounds__(512) integrand_nsx_kernel(const KernelArgs a) 
           const double tP = (log10(z) - sp.l10kT - X.E_min) * X.inv_dE;
           const double fl = floor(tP);
           fP = (float)(tP - fl);
+          if (fP >= 1.f) fP = 0.99999994f;
           G0 = G.iE_min + (int)fl;
           clamped = (G.tE_lo + tP < 0.0) || (G.tE_hi + tP > (double)(nE - 1)) || sp.T_clamped || s_int[45];
           // mu weights (cpu/nsx.hpp:173-321)
           double am;
           const int im = vhunt(s.mu, nmu, mu, am);
-          double w[4] = {0, 0, 0, 0};
-          int start;
           const bool linear_mu = (mode == 4) || ((mode == 2 || mode == 3) && im >= nmu - 5);
+          int start;
           if (linear_mu) {
             start = min(im, nmu - 4);
             const int o = im - start;
-            w[o] = 1 - am;
-            w[o + 1] = am;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) w4[k] = k == o ? (float)(1 - am) : (k == o + 1 ? (float)am : 0.f);
           } else {
             start = clampi(im - 1, 0, nmu - 4);
-            cubic_lagrange(w, mu, s.mu[start], s.mu[start + 1], s.mu[start + 2], s.mu[start + 3]);
+            const double x0 = s.mu[start], x1 = s.mu[start + 1], x2 = s.mu[start + 2], x3 = s.mu[start + 3];
+            const double* r = den + 4 * start;
+            w4[0] = (float)((mu - x1) * (mu - x2) * (mu - x3) * r[0]);
+            w4[1] = (float)((mu - x0) * (mu - x2) * (mu - x3) * r[1]);
+            w4[2] = (float)((mu - x0) * (mu - x1) * (mu - x3) * r[2]);
+            w4[3] = (float)((mu - x0) * (mu - x1) * (mu - x2) * r[3]);
           }
           imu = start;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) w4[k] = (float)w[k];
         }
       }
-      int n_batch;
-      const int slot = block_compact(vis, s_int, &n_batch);
+      int nv;
+      const int slot = block_compact(vis, s_int, &nv);
       if (vis) {
-        b_c[slot] = c;
-        b_fP[slot] = fP;
-        b_G0[slot] = G0;
-        b_bin[slot] = bin;
-        b_imu[slot] = imu;
+        r_pk[slot] = make_float4(c, fP, __int_as_float(bin), __int_as_float(G0));
+        r_imu[slot] = imu;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) b_w[k * S.pb + slot] = w4[k];
+        for (int k = 0; k < 4; ++k) r_w[k * nt + slot] = w4[k];
+        if (clamped) atomicAdd(&s_int[44], 1);
       }
-      if (vis && clamped) atomicAdd(&s_int[44], 1);
       __syncthreads();
       if (tid == 0) {
-        if (n_batch) atomicAdd(&p.stats[3], (unsigned long long)n_batch);
+        if (nv) atomicAdd(&p.stats[3], (unsigned long long)nv);
         if (s_int[44]) atomicAdd(&p.stats[4], (unsigned long long)s_int[44]);
         s_int[44] = 0;
       }
-      __syncthreads();
-      if (n_batch == 0) continue;
 
-      // stage B1: mu-contracted slice rows H[b][kk], k = kH0 + kk
-      for (int idx = tid; idx < n_batch * HN; idx += nt) {
-        const int b = idx / HN, kk = idx - b * HN;
-        const int kH0 = clampi(b_G0[b] - 1, 0, nE - 4);
-        const int k = kH0 + kk;
-        float h = 0.f;
-        if (k < nE) {
-          const float* row = s.S + k * nmu + b_imu[b];
-          h = b_w[b] * row[0];
-          h = fmaf(b_w[S.pb + b], row[1], h);
-          h = fmaf(b_w[2 * S.pb + b], row[2], h);
-          h = fmaf(b_w[3 * S.pb + b], row[3], h);
-        }
-        s.H[idx] = h;
-      }
-      __syncthreads();
-      // stage B2: per-cell polynomials in the cell fraction
-      for (int idx = tid; idx < n_batch * cells; idx += nt) {
-        const int b = idx / cells, cc = idx - b * cells;
-        const int G0b = b_G0[b];
-        const int kH0 = clampi(G0b - 1, 0, nE - 4);
-        const float* H = s.H + b * HN;
-        const int gcell = G0b + cc;
-        float4 Q;
-        if (gcell < 0) {
-          Q = make_float4(H[0 - kH0], 0.f, 0.f, 0.f);
-        } else if (gcell > nE - 2) {
-          Q = make_float4(H[nE - 1 - kH0], 0.f, 0.f, 0.f);
-        } else if (cubicE) {
-          const int ie = clampi(gcell - 1, 0, nE - 4);
-          const int off = gcell - ie;
-          const float h0 = H[ie - kH0], h1 = H[ie - kH0 + 1], h2 = H[ie - kH0 + 2], h3 = H[ie - kH0 + 3];
-          const float d1 = h1 - h0, d2 = h2 - 2.f * h1 + h0, d3 = h3 - 3.f * h2 + 3.f * h1 - h0;
-          const float c3 = d3 * (1.f / 6.f);
-          if (off == 1)
-            Q = make_float4(h1, d1 + 0.5f * d2 - c3, 0.5f * d2, c3);
-          else if (off == 0)
-            Q = make_float4(h0, d1 - 0.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 - 0.5f * d3, c3);
-          else
-            Q = make_float4(h2, d1 + 1.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 + 0.5f * d3, c3);
-        } else {
-          const float h0 = H[gcell - kH0], h1 = H[gcell - kH0 + 1];
-          Q = make_float4(h0, h1 - h0, 0.f, 0.f);
-        }
-        s.Q[idx] = Q;
-      }
-      __syncthreads();
-
-      // stage C: every thread integrates its energies over the batch
-      for (int b = 0; b < n_batch; ++b) {
-        const int bb = b_bin[b];
-        if (bb != cur_bin) {
-          if (cur_bin >= 0) flush();
-          cur_bin = bb;
-        }
-        const float cb = b_c[b], fPb = b_fP[b];
-        const float4* Qb = s.Q + b * cells;
-#pragma unroll
-        for (int k = 0; k < NE_T; ++k) {
-          float tf = fE[k] + fPb;
-          int cidx = rE[k];
-          if (tf >= 1.f) {
-            tf -= 1.f;
-            cidx += 1;
+      for (int s0 = 0; s0 < nv; s0 += S.pb) {
+        const int nb = min(S.pb, nv - s0);
+        // stage B: one warp per point builds the mu-contracted rows H and the
+        // per-cell cubic polynomials Q (Newton form rewritten in the cell fraction)
+        for (int b = warp; b < nb; b += nwarps) {
+          const int rec = s0 + b;
+          const int G0b = __float_as_int(r_pk[rec].w), imb = r_imu[rec];
+          const float w0 = r_w[rec], w1 = r_w[nt + rec], w2 = r_w[2 * nt + rec], w3 = r_w[3 * nt + rec];
+          const int kH0 = clampi(G0b - 1, 0, nE - 4);
+          float* H = s.H + b * HN;
+          for (int kk = lane; kk < HN; kk += 32) {
+            const int k = kH0 + kk;
+            float h = 0.f;
+            if (k < nE) {
+              const float* row = s.S + k * nmu + imb;
+              h = fmaf(w3, row[3], fmaf(w2, row[2], fmaf(w1, row[1], w0 * row[0])));
+            }
+            H[kk] = h;
           }
-          const float4 Qv = Qb[cidx];
-          float it3 = fmaf(fmaf(fmaf(Qv.w, tf, Qv.z), tf, Qv.y), tf, Qv.x);
-          if (sg) it3 = fmaxf(it3, 0.f);
-          acc[k] = fmaf(cb, it3, acc[k]);
+          __syncwarp();
+          float4* Qb = s.Q + b * cells;
+          for (int cc = lane; cc < cells; cc += 32) {
+            const int gcell = G0b + cc;
+            float4 Qv;
+            if (gcell < 0) {
+              Qv = make_float4(H[0 - kH0], 0.f, 0.f, 0.f);
+            } else if (gcell > nE - 2) {
+              Qv = make_float4(H[nE - 1 - kH0], 0.f, 0.f, 0.f);
+            } else if (cubicE) {
+              const int ie = clampi(gcell - 1, 0, nE - 4);
+              const int off = gcell - ie;
+              const float h0 = H[ie - kH0], h1 = H[ie - kH0 + 1], h2 = H[ie - kH0 + 2], h3 = H[ie - kH0 + 3];
+              const float d1 = h1 - h0, d2 = h2 - 2.f * h1 + h0, d3 = h3 - 3.f * h2 + 3.f * h1 - h0;
+              const float c3 = d3 * (1.f / 6.f);
+              if (off == 1)
+                Qv = make_float4(h1, d1 + 0.5f * d2 - c3, 0.5f * d2, c3);
+              else if (off == 0)
+                Qv = make_float4(h0, d1 - 0.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 - 0.5f * d3, c3);
+              else
+                Qv = make_float4(h2, d1 + 1.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 + 0.5f * d3, c3);
+            } else {
+              const float h0 = H[gcell - kH0], h1 = H[gcell - kH0 + 1];
+              Qv = make_float4(h0, h1 - h0, 0.f, 0.f);
+            }
+            Qb[cc] = Qv;
+          }
         }
+        __syncthreads();
+
+        // stage C: every thread integrates its energies over the sub-batch; two
+        // points of the same bin are interleaved for instruction-level parallelism
+        for (int b = 0; b < nb;) {
+          const float4 r0 = r_pk[s0 + b];
+          const int bin0 = __float_as_int(r0.z);
+          if (bin0 != cur_bin) {
+            if (cur_bin >= 0) flush();
+            cur_bin = bin0;
+          }
+          const float4* Q0 = s.Q + b * cells;
+          bool two = false;
+          float4 r1 = r0;
+          if (b + 1 < nb) {
+            r1 = r_pk[s0 + b + 1];
+            two = __float_as_int(r1.z) == bin0;
+          }
+          if (two) {
+            const float4* Q1 = Q0 + cells;
+#pragma unroll
+            for (int k = 0; k < NE_T; ++k) {
+              float t0 = fE[k] + r0.y, t1 = fE[k] + r1.y;
+              const int k0 = t0 >= 1.f, k1 = t1 >= 1.f;
+              t0 = k0 ? t0 - 1.f : t0;
+              t1 = k1 ? t1 - 1.f : t1;
+              const float4 qa = Q0[rE[k] + k0], qb = Q1[rE[k] + k1];
+              float ia = fmaf(fmaf(fmaf(qa.w, t0, qa.z), t0, qa.y), t0, qa.x);
+              float ib = fmaf(fmaf(fmaf(qb.w, t1, qb.z), t1, qb.y), t1, qb.x);
+              if (sg) {
+                ia = fmaxf(ia, 0.f);
+                ib = fmaxf(ib, 0.f);
+              }
+              acc[k] = fmaf(r1.x, ib, fmaf(r0.x, ia, acc[k]));
+            }
+            b += 2;
+          } else {
+#pragma unroll
+            for (int k = 0; k < NE_T; ++k) {
+              float t0 = fE[k] + r0.y;
+              const int k0 = t0 >= 1.f;
+              t0 = k0 ? t0 - 1.f : t0;
+              const float4 qa = Q0[rE[k] + k0];
+              float ia = fmaf(fmaf(fmaf(qa.w, t0, qa.z), t0, qa.y), t0, qa.x);
+              if (sg) ia = fmaxf(ia, 0.f);
+              acc[k] = fmaf(r0.x, ia, acc[k]);
+            }
+            b += 1;
+          }
+        }
+        __syncthreads();
       }
     }
     if (cur_bin >= 0) flush();
@@ -480,9 +508,9 @@ __global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
   __shared__ int s_int[48];
   __shared__ int s_tile;
   const int tid = threadIdx.x, nt = blockDim.x;
-  double* b_c = (double*)s.batch;
-  double* b_z = b_c + S.pb;
-  int* b_bin = (int*)(b_z + S.pb);
+  double* b_c = (double*)s.batch;  // point records, one slot per thread
+  double* b_z = b_c + nt;
+  int* b_bin = (int*)(b_z + nt);
 
   for (;;) {
     __syncthreads();
@@ -521,12 +549,12 @@ __global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
         acc[k] = 0;
       }
     };
-    for (int q0 = 0; q0 < n_pts; q0 += S.pb) {
+    for (int q0 = 0; q0 < n_pts; q0 += nt) {
       bool vis = false;
       double c = 0, zz = 0;
       int bin = 0;
       const int q = q0 + tid;
-      if (tid < S.pb && q < n_pts) {
+      if (q < n_pts) {
         double wgl, z = 0, mu = 0;
         const double flux = phase_point(p, s, tile.ring, point, n_act, q, bin, wgl, z, mu);
         if (flux != 0.0) {
@@ -648,7 +676,7 @@ __global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const De
       if (ring_dropped(p, L, g, nsx)) {
         atomicAdd(&p.stats[1], 1ull);
         atomicAdd(&p.stats[2], 1ull);
-        atomicAdd(&p.stats[0], 1ull);
+        atomicAdd(&p.stats[5], 1ull);
       } else {
         push_tile(q, Tile{pi, (short)si, 1, 0, 0, 1});
       }
@@ -672,7 +700,7 @@ __global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const De
       if (na) {
         atomicAdd(&p.stats[1], 1ull);
         atomicAdd(&p.stats[2], 1ull);
-        atomicAdd(&p.stats[0], (unsigned long long)na);
+        atomicAdd(&p.stats[5], (unsigned long long)na);
         if (g.u_clamped) atomicAdd(&p.stats[4], 1ull);
       }
       continue;
@@ -750,14 +778,14 @@ IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int 
   s.off_MU = off;
   off += al(nf1 * 8);
   s.off_mu = off;
-  off += nsx ? al((long)nmu * 8) : 0;
+  off += nsx ? al((long)nmu * 8 * 5) : 0;
   s.off_S = off;
   // the slice is stored with the table's 16-byte aligned stride
   const long slice = nsx ? ((long)nE * nmu + 3) / 4 * 4 : 0;
   off += al(slice * 4);
   s.off_union = off;
   const int rows = al((long)(4 * n_cp + 2 * n_ca) * 8);
-  const int batch = al((long)pb * kSlotBytes);
+  const int batch = al((long)nt * kSlotBytes);
   const int qbuf = nsx ? al((long)pb * cells * 16) + al((long)pb * (cells + 3) * 4) : 0;
   s.off_rows = off;
   s.off_batch = off;
@@ -768,16 +796,13 @@ IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int 
 }
 
 namespace {
-template <int NE_T>
-void* nsx_fn() {
-  return (void*)integrand_nsx_kernel<NE_T>;
-}
 void* kernel_for(const IntegrandShape& s, int precision) {
   if (s.nsx) {
+    const bool two = s.minb >= 2;
     switch (s.ne_t) {
-      case 1: return nsx_fn<1>();
-      case 2: return nsx_fn<2>();
-      default: return nsx_fn<4>();
+      case 1: return two ? (void*)integrand_nsx_kernel<1, 2> : (void*)integrand_nsx_kernel<1, 1>;
+      case 2: return two ? (void*)integrand_nsx_kernel<2, 2> : (void*)integrand_nsx_kernel<2, 1>;
+      default: return (void*)integrand_nsx_kernel<4, 1>;
     }
   }
   if (precision == 1) {
@@ -799,7 +824,8 @@ cudaError_t configure_integrand_smem(const IntegrandShape& s) {
   // all variants get the largest dynamic shared memory allowance once
   static bool done = false;
   if (done) return cudaSuccess;
-  void* fns[] = {(void*)integrand_nsx_kernel<1>, (void*)integrand_nsx_kernel<2>, (void*)integrand_nsx_kernel<4>,
+  void* fns[] = {(void*)integrand_nsx_kernel<1, 1>, (void*)integrand_nsx_kernel<1, 2>,
+                 (void*)integrand_nsx_kernel<2, 1>, (void*)integrand_nsx_kernel<2, 2>, (void*)integrand_nsx_kernel<4, 1>,
                  (void*)integrand_bb_kernel<double, 1>, (void*)integrand_bb_kernel<double, 2>,
                  (void*)integrand_bb_kernel<double, 4>, (void*)integrand_bb_kernel<float, 1>,
                  (void*)integrand_bb_kernel<float, 2>, (void*)integrand_bb_kernel<float, 4>};

@@ -20,6 +20,7 @@ struct IntegrandShape {
   int cells;      // Q cells per point (span + 1)
   bool nsx;
   int bb_fp64;    // blackbody variant: 1 = FP64 integrand, 0 = FP32
+  int minb;       // CTAs per SM the register budget is compiled for (1 or 2)
   // offsets in bytes
   int off_j, off_P, off_F, off_Z, off_MU, off_mu, off_S, off_union, off_rows, off_batch, off_Q, total;
 };

@@ -114,13 +114,9 @@ class Engine:
             oc += ca[0] * ca[1]
         return out_f, out_c, list(infos)
 
-    def profile_batch_device(self, plist, flux_ptr, counts_ptr, stream=0):
-        """Enqueues a batch whose outputs go to device buffers (integer device pointers)."""
-        n = len(plist)
-        arr = (_abi.Params * n)(*plist)
-        check(lib().ppm_profile_batch_device(self.h, n, arr, None, ctypes.c_void_p(flux_ptr),
-                                             ctypes.c_void_p(counts_ptr) if counts_ptr else None,
-                                             ctypes.c_void_p(stream)))
+    def batch(self, plist):
+        """A device-resident batch: planned once, launched any number of times."""
+        return Batch(self, plist)
 
     # ---- serving
     def submit(self, p, flux, counts):
@@ -142,3 +138,41 @@ class Engine:
         v = ctypes.c_double()
         check(lib().ppm_ticket_latency_us(self.h, ticket, ctypes.byref(v)))
         return v.value
+
+
+class Batch:
+    """Wraps ppm_batch: uploads/plans once; `launch(stream)` replays a CUDA graph
+    of plan -> integrand -> fold; outputs stay on the device until `collect`."""
+
+    def __init__(self, engine, plist):
+        self.engine = engine
+        self.n = len(plist)
+        self.params = (_abi.Params * self.n)(*plist)
+        h = ctypes.c_void_p()
+        check(lib().ppm_batch_create(engine.h, self.n, self.params, ctypes.byref(h)))
+        self.h = h
+        f = ctypes.c_void_p()
+        c = ctypes.c_void_p()
+        nf = ctypes.c_int64()
+        nc = ctypes.c_int64()
+        check(lib().ppm_batch_device_outputs(self.h, ctypes.byref(f), ctypes.byref(nf), ctypes.byref(c),
+                                             ctypes.byref(nc)))
+        self.flux_ptr, self.n_flux, self.counts_ptr, self.n_counts = f.value, nf.value, c.value, nc.value
+
+    def launch(self, stream=0):
+        check(lib().ppm_batch_launch(self.engine.h, self.h, ctypes.c_void_p(stream)))
+
+    def collect(self, want_flux=False, want_counts=True):
+        flux = np.zeros(self.n_flux) if want_flux else None
+        counts = np.zeros(max(self.n_counts, 1)) if want_counts else None
+        infos = (_abi.ResultInfo * self.n)()
+        check(lib().ppm_batch_collect(self.engine.h, self.h, dptr(flux), dptr(counts), infos))
+        return flux, counts, list(infos)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ppm_batch_destroy(self.engine.h, self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

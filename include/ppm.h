@@ -152,6 +152,7 @@ typedef struct ppm_result_info {
   int64_t n_dropped_rings; /* rings skipped because the first/last fine sample is invisible */
   int64_t n_points;        /* visible (element, phase node) pairs that were integrated */
   int64_t n_clamped;       /* lookups clamped to a table edge (u per ring, logEkT per point) */
+  int64_t n_active_integrated; /* active elements on rings that were integrated (not dropped) */
   int32_t status;
   int32_t reserved;
 } ppm_result_info;
@@ -209,11 +210,25 @@ int ppm_profile(ppm_engine* e, const ppm_params* p, double* flux, double* counts
 int ppm_profile_batch(ppm_engine* e, int32_t n, const ppm_params* p, double* flux, double* counts,
                       ppm_result_info* info);
 
-/* Same as ppm_profile_batch with every buffer already in device memory and no
- * host synchronisation: enqueues on `stream` (a cudaStream_t, 0 = engine stream). */
-int ppm_profile_batch_device(ppm_engine* e, int32_t n, const ppm_params* p_host_shapes,
-                             const ppm_params* p_device, double* flux_device, double* counts_device,
-                             void* stream);
+/* Device-resident batches.  ppm_batch_create converts and uploads n profiles,
+ * allocates their device output pools and captures one pass of the kernels
+ * (plan -> integrand -> fold) in a CUDA graph; ppm_batch_launch replays it on
+ * `stream` (a cudaStream_t, NULL = the engine stream) without host
+ * synchronisation; outputs stay in device memory until collected. */
+typedef struct ppm_batch ppm_batch;
+int ppm_batch_create(ppm_engine* e, int32_t n, const ppm_params* p, ppm_batch** out);
+int ppm_batch_launch(ppm_engine* e, ppm_batch* b, void* stream);
+/* Device pointers and sizes (doubles) of the batch's flux and counts pools. */
+int ppm_batch_device_outputs(ppm_batch* b, double** flux, int64_t* n_flux, double** counts, int64_t* n_counts);
+/* Waits for the last launch and copies the outputs to host memory (either may be NULL). */
+int ppm_batch_collect(ppm_engine* e, ppm_batch* b, double* flux, double* counts, ppm_result_info* info);
+void ppm_batch_destroy(ppm_engine* e, ppm_batch* b);
+/* Profiling form of ppm_batch_launch: the same pass launched kernel by kernel
+ * with CUDA events between the phases; waits and returns the device time in
+ * milliseconds of ms[0] = clear + plan, ms[1] = integrand, ms[2] = fold. */
+int ppm_batch_launch_timed(ppm_engine* e, ppm_batch* b, void* stream, float* ms);
+/* Number of engine kernels one pass of the batch launches. */
+int ppm_batch_kernel_count(ppm_engine* e, ppm_batch* b, int32_t* n);
 
 /* Sizes of the output arrays for a parameter set (doubles). */
 int ppm_output_sizes(ppm_engine* e, const ppm_params* p, int64_t* n_flux, int64_t* n_counts);

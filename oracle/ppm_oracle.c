@@ -719,14 +719,18 @@ typedef struct {
   const double* E;
   double* flux;
   size_t stride;
-  int n, next_base, step;
+  int n;
+  int* next; /* shared work counter: profiles are handed out one at a time */
   ppm_result_info* info;
 } batch_job;
 
 static void* batch_worker(void* arg) {
   batch_job* j = (batch_job*)arg;
-  for (int k = j->next_base; k < j->n; k += j->step)
+  for (;;) {
+    int k = __atomic_fetch_add(j->next, 1, __ATOMIC_RELAXED);
+    if (k >= j->n) break;
     oracle_profile(j->c, &j->p[k], j->n_e, j->E, j->flux + (size_t)k * j->stride, j->info ? &j->info[k] : NULL);
+  }
   return NULL;
 }
 
@@ -738,8 +742,9 @@ int oracle_profile_batch(const oracle_ctx* c, int n, const ppm_params* p, int n_
   size_t stride = (size_t)p[0].n_bins * n_e;
   pthread_t th[256];
   batch_job jobs[256];
+  int next = 0;
   for (int t = 0; t < n_threads; ++t) {
-    jobs[t] = (batch_job){c, p, n_e, E, flux, stride, n, t, n_threads, info};
+    jobs[t] = (batch_job){c, p, n_e, E, flux, stride, n, &next, info};
     pthread_create(&th[t], NULL, batch_worker, &jobs[t]);
   }
   for (int t = 0; t < n_threads; ++t) pthread_join(th[t], NULL);
