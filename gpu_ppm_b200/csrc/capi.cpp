@@ -275,6 +275,13 @@ void ppm_batch_destroy(ppm_engine* e, ppm_batch* b) {
   delete reinterpret_cast<ppm::BatchImpl*>(b);
 }
 
+int ppm_profile_noalloc(ppm_engine* e, const ppm_params* p, double* flux_device, double* counts_device, void* stream) {
+  return guarded([&] {
+    if (!p) throw Error(PPM_E_INVALID, "null params");
+    eng(e).profile_noalloc(*p, flux_device, counts_device, (cudaStream_t)stream);
+  });
+}
+
 int ppm_output_sizes(ppm_engine* e, const ppm_params* p, int64_t* n_flux, int64_t* n_counts) {
   return guarded([&] {
     if (!p) throw Error(PPM_E_INVALID, "null params");

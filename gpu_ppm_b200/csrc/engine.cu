@@ -307,10 +307,8 @@ int Engine::add_response(int grid, int n_ch, const double* rsp) {
 
 // (z, cos(acos z), sin(acos z)) of every ring, computed with the host libm as
 // the reference's GenerateHealpixGrid does (cpu/grid.hpp:219-244,254).
-const double* Engine::ring_table(int N) {
-  auto it = ring_tabs.find(N);
-  if (it != ring_tabs.end()) return it->second;
-  std::vector<double> h(3 * (size_t)4 * N, 0.0);
+void compute_ring_rows(int N, std::vector<double>& h) {
+  h.assign(3 * (size_t)4 * N, 0.0);
   for (int i = 1; i <= 4 * N - 1; ++i) {
     int ii = i > 2 * N ? 4 * N - i : i;
     double z = ii < N ? 1. - 1. * ii * ii / (3. * N * N) : 4. / 3. - 2. * ii / (3. * N);
@@ -320,6 +318,23 @@ const double* Engine::ring_table(int N) {
     h[3 * i + 1] = std::cos(th);
     h[3 * i + 2] = std::sin(th);
   }
+}
+
+void compute_fine_rows(int nf, std::vector<double>& h) {
+  h.resize(2 * (size_t)nf);
+  for (int k = 0; k < nf; ++k) {
+    double phase = 1. * k / nf;
+    double spot_phi = two_pi * phase;
+    h[2 * k] = std::cos(spot_phi);
+    h[2 * k + 1] = std::sin(spot_phi);
+  }
+}
+
+const double* Engine::ring_table(int N) {
+  auto it = ring_tabs.find(N);
+  if (it != ring_tabs.end()) return it->second;
+  std::vector<double> h;
+  compute_ring_rows(N, h);
   host_rings[N] = h;
   double* d = dev_upload(h.data(), h.size());
   ring_tabs[N] = d;
@@ -330,13 +345,8 @@ const double* Engine::ring_table(int N) {
 const double* Engine::fine_table(int nf) {
   auto it = fine_tabs.find(nf);
   if (it != fine_tabs.end()) return it->second;
-  std::vector<double> h(2 * (size_t)nf);
-  for (int k = 0; k < nf; ++k) {
-    double phase = 1. * k / nf;
-    double spot_phi = two_pi * phase;
-    h[2 * k] = std::cos(spot_phi);
-    h[2 * k + 1] = std::sin(spot_phi);
-  }
+  std::vector<double> h;
+  compute_fine_rows(nf, h);
   double* d = dev_upload(h.data(), h.size());
   fine_tabs[nf] = d;
   return d;
@@ -378,6 +388,16 @@ void Engine::validate(const ppm_params& p) const {
 }
 
 void Engine::to_device(const ppm_params& p, DevProfile& d, long long flux_off, unsigned long long* stats) {
+  const double* ring = ring_table(p.n_side);
+  const double* fine = fine_table(p.n_fine);
+  prepare_grid(p.energy_grid);
+  fill_profile(p, d, flux_off, stats, ring, fine, dev_grid(p.energy_grid), host_rings[p.n_side]);
+}
+
+// Everything of to_device that needs no device allocation: the ring / fine
+// tables and the energy grid are passed in.
+void Engine::fill_profile(const ppm_params& p, DevProfile& d, long long flux_off, unsigned long long* stats,
+                          const double* ring, const double* fine, const DevGrid& grid, const std::vector<double>& rt) {
   std::memset(&d, 0, sizeof(d));
   // cpu/devarshi24st_cpu.cpp:48-74
   const double M = p.mass_msun, Re = p.r_eq_km, frequency_nu = p.spin_hz;
@@ -421,14 +441,12 @@ void Engine::to_device(const ppm_params& p, DevProfile& d, long long flux_off, u
   d.beaming = p.beaming;
   d.precision = p.precision;
   d.flux_off = flux_off;
-  d.ring = ring_table(p.n_side);
-  d.fine = fine_table(p.n_fine);
-  prepare_grid(p.energy_grid);
-  d.grid = dev_grid(p.energy_grid);
+  d.ring = ring;
+  d.fine = fine;
+  d.grid = grid;
   d.n_e = d.grid.n_e;
   d.stats = stats;
   const bool nsx_atm = p.atmosphere == PPM_ATM_NSX;
-  const std::vector<double>& rt = host_rings[p.n_side];
   for (int s = 0; s < p.n_spots; ++s) {
     const ppm_spot& sp = p.spots[s];
     DevSpot& o = d.spot[s];

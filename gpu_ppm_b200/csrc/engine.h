@@ -20,6 +20,10 @@
 
 namespace ppm {
 
+// Host rows of the per-N_side ring table and the per-n_fine phase table.
+void compute_ring_rows(int N, std::vector<double>& h);
+void compute_fine_rows(int nf, std::vector<double>& h);
+
 struct Error : std::runtime_error {
   int code;
   Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
@@ -135,6 +139,7 @@ class Engine {
   int kernels_per_pass(const BatchImpl& B) const;
   void batch_launch_timed(BatchImpl& B, cudaStream_t st, float* ms);
   void output_sizes(const ppm_params& p, int64_t* n_flux, int64_t* n_counts) const;
+  void profile_noalloc(const ppm_params& p, double* flux_d, double* counts_d, cudaStream_t st);
 
   // serving
   uint64_t submit(const ppm_params& p, double* flux, double* counts);
@@ -152,6 +157,8 @@ class Engine {
   friend struct Server;
   void validate(const ppm_params& p) const;
   void to_device(const ppm_params& p, DevProfile& d, long long flux_off, unsigned long long* stats);
+  void fill_profile(const ppm_params& p, DevProfile& d, long long flux_off, unsigned long long* stats,
+                    const double* ring, const double* fine, const DevGrid& grid, const std::vector<double>& rt);
   void prepare_grid(int id);
   DevGrid dev_grid(int id);
   const double* ring_table(int N);

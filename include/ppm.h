@@ -230,6 +230,22 @@ int ppm_batch_launch_timed(ppm_engine* e, ppm_batch* b, void* stream, float* ms)
 /* Number of engine kernels one pass of the batch launches. */
 int ppm_batch_kernel_count(ppm_engine* e, ppm_batch* b, int32_t* n);
 
+/* Allocation-free plain form, for callers that may not allocate device memory
+ * while they run (a sampler that reserved the whole GPU for its own pool at
+ * start-up, a framework whose caching allocator owns the device, or a loop
+ * where cudaMalloc's implicit device synchronisation would stall other
+ * streams).  No counterpart in the reference: it has no allocation-free path.
+ * Enqueues one profile on `stream` (a cudaStream_t, NULL = engine stream) and
+ * returns without waiting; flux_device [n_bins][n_e] (required) and
+ * counts_device [n_ch][n_bins] (optional) are caller-owned device buffers.
+ * All other working state lives in one 1 MiB device array that the library
+ * declares statically (held on every device that loads the library until
+ * process exit); profiles whose tables and work queue do not fit — about
+ * N_side > 512 with two spots — are rejected with PPM_E_RANGE.  The first call
+ * on a device looks up the array's address; make it before any stream capture.
+ * Calls share the array, so calls that overlap on the GPU race. */
+int ppm_profile_noalloc(ppm_engine* e, const ppm_params* p, double* flux_device, double* counts_device, void* stream);
+
 /* Sizes of the output arrays for a parameter set (doubles). */
 int ppm_output_sizes(ppm_engine* e, const ppm_params* p, int64_t* n_flux, int64_t* n_counts);
 
