@@ -110,12 +110,15 @@ Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   if (const char* v = std::getenv("PPM_NE_T")) tune.ne_t = std::atoi(v);
   if (const char* v = std::getenv("PPM_MINB")) tune.minb = std::max(1, std::min(2, std::atoi(v)));
   for (int k = 0; k < 4; ++k) PPM_CUDA(cudaEventCreate(&ev[k]));
+  PPM_CUDA(cudaMalloc(&d_err, sizeof(int)));
+  PPM_CUDA(cudaMemset(d_err, 0, sizeof(int)));
 }
 
 Engine::~Engine() {
   cudaSetDevice(cfg.device);
   serve_shutdown();
   cudaStreamSynchronize(stream);
+  if (d_err) cudaFree(d_err);
   for (void* p : owned) cudaFree(p);
   for (auto& kv : ring_tabs) cudaFree(kv.second);
   for (auto& kv : fine_tabs) cudaFree(kv.second);
@@ -731,6 +734,12 @@ void Engine::batch_collect(BatchImpl& B, double* flux, double* counts, ppm_resul
   PPM_CUDA(cudaStreamSynchronize(st));
   PPM_CUDA(cudaGetLastError());
   if (ctrl[2] || ctrl[5] || ctrl[8]) throw Error(PPM_E_RANGE, "work queue overflow");
+  int err = 0;
+  PPM_CUDA(cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    PPM_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+    throw Error(PPM_E_TIMEOUT, "a bounded wait in the tensor-core fold ran out");
+  }
   if (info) {
     for (int i = 0; i < n; ++i) {
       ppm_result_info& r = info[i];

@@ -181,6 +181,7 @@ class Engine {
   std::map<int, std::vector<double>> host_rings;
   std::vector<void*> owned;
   cudaEvent_t ev[4];
+  int* d_err = nullptr;  // set by kernels whose bounded waits ran out
 
   // serving state
   struct Server* server = nullptr;

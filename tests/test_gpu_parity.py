@@ -143,3 +143,32 @@ def test_batch_matches_plain(eng_v171019):
     for k in range(3):
         ref, _ = eng_v171019.ora.profile(plist[k], E)
         assert max_rel(flux_b[k], ref) < TOL32, k
+
+
+def test_fold_precision_config3_shapes():
+    """Config-3 response shape (1500 channels from a 3000-bin fine grid, 300
+    energies, 128 bins): FP64 SIMT, FP32 SIMT and BF16x3 tensor-core folds of
+    the same flux against the FP64 oracle fold."""
+    lens, nsx = synth.lensing("std"), synth.nsx("v171019", seed=0)
+    e = Engine()
+    e.load_lensing(lens)
+    e.load_nsx(nsx)
+    E = synth.energy_grid(300, 0.2, 12.0)
+    g = e.add_energy_grid(E)
+    rsp = synth.response(1500, 3000, E, seed=0)
+    r = e.add_response(g, rsp)
+    p = synth.config3_params(g, r)
+    p.n_side = 48
+    errs = {}
+    flux0 = None
+    for fold in (_abi.FOLD_FP64, _abi.FOLD_FP32, _abi.FOLD_BF16X3):
+        p.fold = fold
+        flux, counts, _ = e.profile(p)
+        if flux0 is None:
+            flux0 = flux
+        ref = oracle.fold(rsp, flux, p.exposure_s)
+        errs[fold] = max_rel(counts, ref)
+    assert errs[_abi.FOLD_FP64] < 1e-12
+    assert errs[_abi.FOLD_FP32] < 1e-5
+    assert errs[_abi.FOLD_BF16X3] < TOL32
+    e.close()
