@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
     return ap.parse_args()
 
 
@@ -369,6 +370,11 @@ def main():
         ev_plain = sum(n_eval(infos[i], plist[i], len(E)) for i in range(n_plain))
         plain_equiv = n / (evals / (ev_plain / t_plain)) if ev_plain else None  # same mix, scaled by evaluations
 
+    # ---- serving: continuous batching under open-loop request streams (rank 0, N = 1)
+    served = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        served = serving_bench(lens, nsx, synth, _abi, Engine, local)
+
     # ---- CPU baseline (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -406,6 +412,10 @@ def main():
             "gpu_launches": kcount.value * args.steps,
             "clocks": clocks,
         }
+        if served:
+            line["served"] = {"requests": "random-walk sampler proposals, N_side {64,128,256,512}, bins {32,64,128}, "
+                                          "energies {128,300}, channels {300,1500}, open-loop Poisson arrivals",
+                              "runs": served, "p50_ms": served[0]["p50_ms"], "p99_ms": served[0]["p99_ms"]}
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -413,6 +423,81 @@ def main():
         dist.barrier()
         dist.destroy_process_group()
     eng.close()
+
+
+def random_walk_requests(n, seed, grids, synth, abi):
+    """Proposals of a random-walk sampler over the batching prior (step 1% of each
+    range, reflected at the bounds) with mixed request sizes: N_side in
+    {64,128,256,512}, phase bins in {32,64,128}, energy grids {128,300} and 300- or
+    1500-channel responses."""
+    rng = np.random.default_rng(seed)
+    lo = np.array([1.0, 9.0, 100.0, 5.0, 0.0, 0.0, math.log(0.01), 5.8])
+    hi = np.array([2.2, 15.0, 700.0, 90.0, 180.0, 360.0, 0.0, 6.6])
+    start, _ = synth.draw_prior(1, seed=seed, lens_u=(0.15, 0.55))
+    p0 = start[0]
+    sp0 = p0.spots[0]
+    x = np.array([p0.mass_msun, p0.r_eq_km, p0.spin_hz, p0.inclination_rad / synth.DEG, sp0.theta1 / synth.DEG,
+                  (sp0.phi1 / synth.DEG) % 360.0, math.log(sp0.angrad1), sp0.logT])
+    out = []
+    while len(out) < n:
+        y = x + rng.normal(0, 0.01, size=8) * (hi - lo)
+        y = np.where(y < lo, 2 * lo - y, y)
+        y = np.where(y > hi, 2 * hi - y, y)
+        (u_eq, g_eq), (u_po, g_po) = synth.star_u_logg(y[0], y[1], y[2])
+        if 0.15 <= min(u_eq, u_po) and max(u_eq, u_po) <= 0.55 and 13.7 <= min(g_eq, g_po) and max(g_eq, g_po) <= 14.7:
+            x = y
+        ne = int(rng.choice([128, 300]))
+        g, rs = grids[ne]
+        n_bins = int(rng.choice([32, 64, 128]))
+        rho = math.exp(x[6])
+        spot = synth.spot(x[4] * synth.DEG, x[5] * synth.DEG, rho, x[4] * synth.DEG - 0.3 * rho, x[5] * synth.DEG,
+                          0.6 * rho, logT=x[7])
+        out.append(synth.params(mass_msun=x[0], r_eq_km=x[1], spin_hz=x[2], inclination_rad=x[3] * synth.DEG,
+                                distance_kpc=0.15, spots=[spot], atmosphere=abi.ATM_NSX,
+                                interp=abi.INTERP_2L2C_LE, n_side=int(rng.choice([64, 128, 256, 512])),
+                                n_bins=n_bins, n_gl=2, energy_grid=g, response=rs[int(rng.choice([300, 1500]))],
+                                fold=abi.FOLD_BF16X3))
+    return out
+
+
+def serving_bench(lens, nsx, synth, abi, Engine, device, rates=((2000.0, 800), (100.0, 200))):
+    """Open-loop Poisson request streams through ppm_submit (continuous batching)."""
+    eng = Engine(device=device, n_streams=4)
+    eng.load_lensing(lens)
+    eng.load_nsx(nsx)
+    grids = {}
+    for ne in (128, 300):
+        E = synth.energy_grid(ne, 0.2, 12.0)
+        g = eng.add_energy_grid(E)
+        grids[ne] = (g, {ch: eng.add_response(g, synth.response(ch, 1000 if ch == 300 else 3000, E, seed=0))
+                         for ch in (300, 1500)})
+    results = []
+    warm = random_walk_requests(16, 99, grids, synth, abi)
+    for p in warm:  # first-use tables and launch shapes
+        eng.profile(p, want_flux=False)
+    for k, (rate, n) in enumerate(rates):
+        reqs = random_walk_requests(n, 1000 + k, grids, synth, abi)
+        rng = np.random.default_rng(k)
+        t_arr = np.cumsum(rng.exponential(1.0 / rate, size=n))
+        bufs, tickets = [], []
+        t0 = time.perf_counter()
+        for p, ta in zip(reqs, t_arr):
+            while time.perf_counter() - t0 < ta:
+                pass
+            cs = eng.sizes(p)[1]
+            counts = np.zeros(cs)
+            bufs.append(counts)
+            tickets.append(eng.submit(p, None, counts))
+        lat = []
+        for t in tickets:
+            eng.wait(t)
+            lat.append(eng.latency_us(t) / 1000.0)
+        t_all = time.perf_counter() - t0
+        results.append({"offered_req_per_s": rate, "requests": n, "throughput_req_per_s": n / t_all,
+                        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                        "max_ms": float(np.max(lat))})
+    eng.close()
+    return results
 
 
 def cpu_baseline(plist, infos, E, lens, nsx, args):

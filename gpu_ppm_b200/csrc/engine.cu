@@ -61,14 +61,20 @@ void DeviceBuffer::reserve(size_t bytes) {
 }
 void* DeviceArena::alloc(size_t bytes) {
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 16));
+  cudaError_t e = stream ? cudaMallocAsync(&p, std::max<size_t>(bytes, 16), stream)
+                         : cudaMalloc(&p, std::max<size_t>(bytes, 16));
   if (e != cudaSuccess) throw Error(PPM_E_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
   ptrs.push_back(p);
   bytes_held += bytes;
   return p;
 }
 DeviceArena::~DeviceArena() {
-  for (void* p : ptrs) cudaFree(p);
+  for (void* p : ptrs) {
+    if (stream)
+      cudaFreeAsync(p, stream);
+    else
+      cudaFree(p);
+  }
 }
 BatchImpl::~BatchImpl() {
   if (graph) cudaGraphExecDestroy(graph);
@@ -540,7 +546,7 @@ void Engine::fill_profile(const ppm_params& p, DevProfile& d, long long flux_off
 // ---- batches ----------------------------------------------------------------------
 // Converts and uploads n profiles, sizes the work queue and output pools, and
 // records the launch shapes; the batch owns all of its device memory.
-void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps) {
+void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t copy_stream) {
   if (n < 1) throw Error(PPM_E_INVALID, "empty batch");
   if (n > cfg.max_batch) throw Error(PPM_E_RANGE, "batch larger than max_batch");
   PPM_CUDA(cudaSetDevice(cfg.device));
@@ -593,7 +599,10 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps) {
   B.d_counts = (double*)B.mem.alloc(sizeof(double) * (size_t)std::max(1ll, B.counts_off[n]));
   Tile* tiles = (Tile*)B.mem.alloc(sizeof(Tile) * (size_t)std::max(1ll, cap_total));
   B.d_ctrl = (int*)B.mem.alloc(sizeof(int) * 16);
-  PPM_CUDA(cudaMemcpy(B.d_prof, hp.data(), sizeof(DevProfile) * (size_t)n, cudaMemcpyHostToDevice));
+  if (copy_stream)  // pageable source: returns once staged, ordered on the batch's stream
+    PPM_CUDA(cudaMemcpyAsync(B.d_prof, hp.data(), sizeof(DevProfile) * (size_t)n, cudaMemcpyHostToDevice, copy_stream));
+  else
+    PPM_CUDA(cudaMemcpy(B.d_prof, hp.data(), sizeof(DevProfile) * (size_t)n, cudaMemcpyHostToDevice));
   B.h2d_bytes = sizeof(DevProfile) * (size_t)n;
   long long base = 0;
   B.groups.clear();
@@ -646,7 +655,11 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps) {
   }
   if (!jobs.empty()) {
     B.d_jobs = (FoldJob*)B.mem.alloc(sizeof(FoldJob) * jobs.size());
-    PPM_CUDA(cudaMemcpy(B.d_jobs, jobs.data(), sizeof(FoldJob) * jobs.size(), cudaMemcpyHostToDevice));
+    if (copy_stream)
+      PPM_CUDA(cudaMemcpyAsync(B.d_jobs, jobs.data(), sizeof(FoldJob) * jobs.size(), cudaMemcpyHostToDevice,
+                               copy_stream));
+    else
+      PPM_CUDA(cudaMemcpy(B.d_jobs, jobs.data(), sizeof(FoldJob) * jobs.size(), cudaMemcpyHostToDevice));
     B.h2d_bytes += sizeof(FoldJob) * jobs.size();
   }
 }

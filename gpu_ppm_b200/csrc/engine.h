@@ -69,6 +69,7 @@ struct Resp {
 struct DeviceArena {
   std::vector<void*> ptrs;
   size_t bytes_held = 0;
+  cudaStream_t stream = nullptr;  // set: stream-ordered allocations (no implicit device synchronisation)
   void* alloc(size_t bytes);
   DeviceArena() = default;
   DeviceArena(const DeviceArena&) = delete;
@@ -131,7 +132,9 @@ class Engine {
 
   void profile(const ppm_params& p, double* flux, double* counts, ppm_result_info* info);
   void profile_batch(int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info);
-  void batch_build(BatchImpl& B, int n, const ppm_params* ps);
+  void batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t copy_stream = nullptr);
+  size_t request_bytes(const ppm_params& p) const;
+  void warm_tables(const ppm_params& p);
   void batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events);
   void batch_capture(BatchImpl& B);
   void batch_launch(BatchImpl& B, cudaStream_t st);
