@@ -125,6 +125,7 @@ SIGNATURES = {
     "ppm_batch_launch_timed": (c_int32, [c_void_p, c_void_p, c_void_p, POINTER(ctypes.c_float)]),
     "ppm_batch_kernel_count": (c_int32, [c_void_p, c_void_p, POINTER(c_int32)]),
     "ppm_profile_noalloc": (c_int32, [c_void_p, POINTER(Params), c_void_p, c_void_p, c_void_p]),
+    "ppm_engine_autotune": (c_int32, [c_void_p, c_int32, POINTER(Params), c_char_p, c_int32]),
     "ppm_output_sizes": (c_int32, [c_void_p, POINTER(Params), POINTER(c_int64), POINTER(c_int64)]),
     "ppm_submit": (c_int32, [c_void_p, POINTER(Params), DP, DP, POINTER(c_uint64)]),
     "ppm_poll": (c_int32, [c_void_p, c_uint64, POINTER(c_int32)]),

@@ -1,6 +1,7 @@
 // extern "C" entry points of include/ppm.h and the reference text-table readers.
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <fstream>
 #include <limits>
 #include <string>
@@ -279,6 +280,18 @@ int ppm_profile_noalloc(ppm_engine* e, const ppm_params* p, double* flux_device,
   return guarded([&] {
     if (!p) throw Error(PPM_E_INVALID, "null params");
     eng(e).profile_noalloc(*p, flux_device, counts_device, (cudaStream_t)stream);
+  });
+}
+
+int ppm_engine_autotune(ppm_engine* e, int32_t n, const ppm_params* sample, char* report, int32_t report_len) {
+  return guarded([&] {
+    if (!sample || n < 1) throw Error(PPM_E_INVALID, "autotune needs sample profiles");
+    std::string r = eng(e).autotune(n, sample);
+    if (report && report_len > 0) {
+      size_t k = std::min((size_t)report_len - 1, r.size());
+      std::memcpy(report, r.data(), k);
+      report[k] = 0;
+    }
   });
 }
 

@@ -812,6 +812,64 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
   return s;
 }
 
+// Coordinate descent over the integrand's launch shape on a sample batch.
+std::string Engine::autotune(int n, const ppm_params* sample) {
+  std::lock_guard<std::mutex> lk(mu);
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  const Tuning start = tune;
+  auto measure = [&](const Tuning& t) -> float {
+    tune = t;
+    BatchImpl B;
+    batch_build(B, n, sample);
+    batch_enqueue(B, stream, nullptr);  // warm-up
+    PPM_CUDA(cudaEventRecord(ev[0], stream));
+    for (int r = 0; r < 2; ++r) batch_enqueue(B, stream, nullptr);
+    PPM_CUDA(cudaEventRecord(ev[1], stream));
+    PPM_CUDA(cudaEventSynchronize(ev[1]));
+    float ms = 0;
+    PPM_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    return ms / 2;
+  };
+  std::string rep;
+  auto line = [&](const Tuning& t, float ms, const char* note) {
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "pb=%d chunk=%d minb=%d ne_t=%d : %.3f ms%s\n", t.pb, t.chunk, t.minb, t.ne_t, ms,
+                  note);
+    rep += buf;
+  };
+  Tuning best = start;
+  float best_ms = measure(best);
+  line(best, best_ms, " (start)");
+  const std::vector<std::pair<int Tuning::*, std::vector<int>>> dims = {
+      {&Tuning::pb, {10, 20, 30, 40}},
+      {&Tuning::chunk, {256, 512, 1024, 2048}},
+      {&Tuning::minb, {1, 2}},
+      {&Tuning::ne_t, {0, 2}},
+  };
+  for (const auto& d : dims) {
+    for (int v : d.second) {
+      Tuning t = best;
+      if (t.*(d.first) == v) continue;
+      t.*(d.first) = v;
+      float ms;
+      try {
+        ms = measure(t);
+      } catch (const Error& e) {
+        line(t, -1.0f, " (does not fit)");
+        continue;
+      }
+      line(t, ms, "");
+      if (ms < 0.98f * best_ms) {
+        best = t;
+        best_ms = ms;
+      }
+    }
+  }
+  tune = best;
+  line(best, best_ms, " (chosen)");
+  return rep;
+}
+
 void Engine::output_sizes(const ppm_params& p, int64_t* n_flux, int64_t* n_counts) const {
   validate(p);
   if (n_flux) *n_flux = (int64_t)p.n_bins * (int64_t)grids[p.energy_grid].E.size();

@@ -143,6 +143,7 @@ class Engine {
   void batch_launch_timed(BatchImpl& B, cudaStream_t st, float* ms);
   void output_sizes(const ppm_params& p, int64_t* n_flux, int64_t* n_counts) const;
   void profile_noalloc(const ppm_params& p, double* flux_d, double* counts_d, cudaStream_t st);
+  std::string autotune(int n, const ppm_params* sample);
 
   // serving
   uint64_t submit(const ppm_params& p, double* flux, double* counts);

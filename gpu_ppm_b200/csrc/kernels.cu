@@ -398,47 +398,62 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 320, MINB) integrand_nsx_ker
         const int nb = min(S.pb, nv - s0);
         // stage B: one warp per point builds the mu-contracted rows H and the
         // per-cell cubic polynomials Q (Newton form rewritten in the cell fraction)
-        for (int b = warp; b < nb; b += nwarps) {
-          const int rec = s0 + b;
-          const int G0b = __float_as_int(r_pk[rec].w), imb = r_imu[rec];
-          const float w0 = r_w[rec], w1 = r_w[nt + rec], w2 = r_w[2 * nt + rec], w3 = r_w[3 * nt + rec];
-          const int kH0 = clampi(G0b - 1, 0, nE - 4);
-          float* H = s.H + b * HN;
+        for (int b = warp; b < nb; b += 2 * nwarps) {
+          // two points per warp, interleaved for instruction-level parallelism
+          const int bB = b + nwarps;
+          const bool has2 = bB < nb;
+          const int recA = s0 + b, recB = s0 + (has2 ? bB : b);
+          const int G0a = __float_as_int(r_pk[recA].w), G0b = __float_as_int(r_pk[recB].w);
+          const int ima = r_imu[recA], imb = r_imu[recB];
+          const float wa0 = r_w[recA], wa1 = r_w[nt + recA], wa2 = r_w[2 * nt + recA], wa3 = r_w[3 * nt + recA];
+          const float wb0 = r_w[recB], wb1 = r_w[nt + recB], wb2 = r_w[2 * nt + recB], wb3 = r_w[3 * nt + recB];
+          const int kHa = clampi(G0a - 1, 0, nE - 4), kHb = clampi(G0b - 1, 0, nE - 4);
+          float* Ha = s.H + b * HN;
+          float* Hb = s.H + bB * HN;
           for (int kk = lane; kk < HN; kk += 32) {
-            const int k = kH0 + kk;
-            float h = 0.f;
-            if (k < nE) {
-              const float* row = s.S + k * nmu + imb;
-              h = fmaf(w3, row[3], fmaf(w2, row[2], fmaf(w1, row[1], w0 * row[0])));
+            const int ka = kHa + kk, kb = kHb + kk;
+            float ha = 0.f, hb = 0.f;
+            if (ka < nE) {
+              const float* row = s.S + ka * nmu + ima;
+              ha = fmaf(wa3, row[3], fmaf(wa2, row[2], fmaf(wa1, row[1], wa0 * row[0])));
             }
-            H[kk] = h;
+            if (has2 && kb < nE) {
+              const float* row = s.S + kb * nmu + imb;
+              hb = fmaf(wb3, row[3], fmaf(wb2, row[2], fmaf(wb1, row[1], wb0 * row[0])));
+            }
+            Ha[kk] = ha;
+            if (has2) Hb[kk] = hb;
           }
           __syncwarp();
-          float4* Qb = s.Q + b * cells;
-          for (int cc = lane; cc < cells; cc += 32) {
-            const int gcell = G0b + cc;
-            float4 Qv;
-            if (gcell < 0) {
-              Qv = make_float4(H[0 - kH0], 0.f, 0.f, 0.f);
-            } else if (gcell > nE - 2) {
-              Qv = make_float4(H[nE - 1 - kH0], 0.f, 0.f, 0.f);
-            } else if (cubicE) {
-              const int ie = clampi(gcell - 1, 0, nE - 4);
-              const int off = gcell - ie;
-              const float h0 = H[ie - kH0], h1 = H[ie - kH0 + 1], h2 = H[ie - kH0 + 2], h3 = H[ie - kH0 + 3];
-              const float d1 = h1 - h0, d2 = h2 - 2.f * h1 + h0, d3 = h3 - 3.f * h2 + 3.f * h1 - h0;
-              const float c3 = d3 * (1.f / 6.f);
-              if (off == 1)
-                Qv = make_float4(h1, d1 + 0.5f * d2 - c3, 0.5f * d2, c3);
-              else if (off == 0)
-                Qv = make_float4(h0, d1 - 0.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 - 0.5f * d3, c3);
-              else
-                Qv = make_float4(h2, d1 + 1.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 + 0.5f * d3, c3);
-            } else {
-              const float h0 = H[gcell - kH0], h1 = H[gcell - kH0 + 1];
-              Qv = make_float4(h0, h1 - h0, 0.f, 0.f);
+          for (int pt = 0; pt < (has2 ? 2 : 1); ++pt) {
+            const int G0x = pt ? G0b : G0a, kH0 = pt ? kHb : kHa;
+            const float* H = pt ? Hb : Ha;
+            float4* Qb = s.Q + (pt ? bB : b) * cells;
+            for (int cc = lane; cc < cells; cc += 32) {
+              const int gcell = G0x + cc;
+              float4 Qv;
+              if (gcell < 0) {
+                Qv = make_float4(H[0 - kH0], 0.f, 0.f, 0.f);
+              } else if (gcell > nE - 2) {
+                Qv = make_float4(H[nE - 1 - kH0], 0.f, 0.f, 0.f);
+              } else if (cubicE) {
+                const int ie = clampi(gcell - 1, 0, nE - 4);
+                const int off = gcell - ie;
+                const float h0 = H[ie - kH0], h1 = H[ie - kH0 + 1], h2 = H[ie - kH0 + 2], h3 = H[ie - kH0 + 3];
+                const float d1 = h1 - h0, d2 = h2 - 2.f * h1 + h0, d3 = h3 - 3.f * h2 + 3.f * h1 - h0;
+                const float c3 = d3 * (1.f / 6.f);
+                if (off == 1)
+                  Qv = make_float4(h1, d1 + 0.5f * d2 - c3, 0.5f * d2, c3);
+                else if (off == 0)
+                  Qv = make_float4(h0, d1 - 0.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 - 0.5f * d3, c3);
+                else
+                  Qv = make_float4(h2, d1 + 1.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 + 0.5f * d3, c3);
+              } else {
+                const float h0 = H[gcell - kH0], h1 = H[gcell - kH0 + 1];
+                Qv = make_float4(h0, h1 - h0, 0.f, 0.f);
+              }
+              Qb[cc] = Qv;
             }
-            Qb[cc] = Qv;
           }
         }
         __syncthreads();

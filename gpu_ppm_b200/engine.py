@@ -114,6 +114,14 @@ class Engine:
             oc += ca[0] * ca[1]
         return out_f, out_c, list(infos)
 
+    def autotune(self, plist):
+        """Times candidate integrand launch shapes on these profiles and keeps the fastest."""
+        n = len(plist)
+        arr = (_abi.Params * n)(*plist)
+        buf = ctypes.create_string_buffer(8192)
+        check(lib().ppm_engine_autotune(self.h, n, arr, buf, len(buf)))
+        return buf.value.decode()
+
     def batch(self, plist):
         """A device-resident batch: planned once, launched any number of times."""
         return Batch(self, plist)

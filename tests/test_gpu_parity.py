@@ -172,3 +172,32 @@ def test_fold_precision_config3_shapes():
     assert errs[_abi.FOLD_FP32] < 1e-5
     assert errs[_abi.FOLD_BF16X3] < TOL32
     e.close()
+
+
+def test_chunked_rings_and_small_batches(monkeypatch):
+    """Rings split into many work tiles (32 candidate elements each) and small
+    polynomial sub-batches give the oracle's result."""
+    monkeypatch.setenv("PPM_CHUNK", "32")
+    monkeypatch.setenv("PPM_PB", "10")
+    lens, nsx = synth.lensing("std"), synth.nsx("v171019", seed=0)
+    e = Engine()
+    e.load_lensing(lens)
+    e.load_nsx(nsx)
+    E = synth.energy_grid(128, 0.2, 12.0)
+    g = e.add_energy_grid(E)
+    p = synth.config2_params(g, -1, n_side=40, n_bins=16)
+    flux, _, info = e.profile(p, want_counts=False)
+    ref, oinfo = oracle.Oracle(lens, nsx).profile(p, E)
+    assert info.n_active == oinfo.n_active and info.n_points == oinfo.n_points
+    assert max_rel(flux, ref) < TOL32
+    e.close()
+
+
+def test_autotune_keeps_parity(eng_v171019):
+    g, r, E, rsp = eng_v171019.cfg2
+    plist, _ = synth.draw_prior(8, seed=21, lens_u=(0.3, 0.5), n_side=32, n_bins=16, energy_grid=g, response=r)
+    report = eng_v171019.autotune(plist)
+    assert "(chosen)" in report
+    f, c, _ = eng_v171019.profile(plist[0])
+    ref, _ = eng_v171019.ora.profile(plist[0], E)
+    assert max_rel(f, ref) < TOL32
