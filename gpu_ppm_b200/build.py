@@ -9,6 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libppm_b200.so")
+RUN = os.path.join(OUT_DIR, "ppm_run")
 
 SOURCES = ["kernels.cu", "fold_tc.cu", "engine.cu", "noalloc.cu", "capi.cpp", "serve.cpp", "lensgen.cpp", "util.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -20,7 +21,7 @@ def _needs_build():
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "ppm.h"), __file__]
-    return any(os.path.getmtime(d) > t for d in deps)
+    return not os.path.exists(RUN) or any(os.path.getmtime(d) > t for d in deps)
 
 
 def build(force=False, verbose=False):
@@ -49,6 +50,10 @@ def build(force=False, verbose=False):
     tmp = LIB + f".{os.getpid()}.tmp"
     subprocess.run([NVCC, "-shared", *ARCH, "-o", tmp, *objs, "-lpthread"], check=True)
     os.replace(tmp, LIB)
+    # the drop-in driver links the library from its own directory
+    subprocess.run(["g++", "-std=c++17", "-O2", os.path.join(CSRC, "ppm_run.cpp"), "-o", RUN + ".tmp",
+                    f"-L{OUT_DIR}", "-lppm_b200", "-Wl,-rpath,$ORIGIN"], check=True)
+    os.replace(RUN + ".tmp", RUN)
     return LIB
 
 
