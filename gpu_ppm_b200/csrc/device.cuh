@@ -47,6 +47,12 @@ struct DevGrid {
   const double* invE;
   const int* rE;    // floor(t_E) - iE_min
   const float* fE;  // t_E - floor(t_E)
+  // energies grouped by home cell rE (ascending t_E): the energies of home cell r
+  // are perm[cell_first[r] .. cell_first[r + 1]), their fractions fEs[same range]
+  const int* perm;        // [n_e] energy index in t_E order
+  const float* fEs;       // [n_e] fE in t_E order
+  const int* cell_first;  // [span + 1]
+  int maxe;               // most energies in one home cell
 };
 
 struct DevSpot {

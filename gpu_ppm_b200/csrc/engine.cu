@@ -110,11 +110,13 @@ Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   PPM_CUDA(cudaSetDevice(cfg.device));
   PPM_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, cfg.device));
   PPM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-  // launch-shape overrides for experiments: PPM_PB, PPM_CHUNK, PPM_NE_T, PPM_MINB
+  // launch-shape overrides for experiments: PPM_PB, PPM_CHUNK, PPM_NE_T, PPM_MINB, PPM_KERNEL, PPM_SETS
   if (const char* v = std::getenv("PPM_PB")) tune.pb = std::max(1, std::atoi(v));
   if (const char* v = std::getenv("PPM_CHUNK")) tune.chunk = std::max(32, std::atoi(v));
   if (const char* v = std::getenv("PPM_NE_T")) tune.ne_t = std::atoi(v);
-  if (const char* v = std::getenv("PPM_MINB")) tune.minb = std::max(1, std::min(2, std::atoi(v)));
+  if (const char* v = std::getenv("PPM_MINB")) tune.minb = std::max(1, std::min(3, std::atoi(v)));
+  if (const char* v = std::getenv("PPM_KERNEL")) tune.kernel = std::atoi(v) ? 1 : 0;
+  if (const char* v = std::getenv("PPM_SETS")) tune.sets = std::max(0, std::atoi(v));
   for (int k = 0; k < 4; ++k) PPM_CUDA(cudaEventCreate(&ev[k]));
   PPM_CUDA(cudaMalloc(&d_err, sizeof(int)));
   PPM_CUDA(cudaMemset(d_err, 0, sizeof(int)));
@@ -128,6 +130,9 @@ Engine::~Engine() {
   for (void* p : owned) cudaFree(p);
   for (auto& kv : ring_tabs) cudaFree(kv.second);
   for (auto& kv : fine_tabs) cudaFree(kv.second);
+  for (const Grid& g : grids)
+    for (void* q : {(void*)g.drE, (void*)g.dfE, (void*)g.dperm, (void*)g.dfEs, (void*)g.dcell_first})
+      if (q) cudaFree(q);
   for (int k = 0; k < 4; ++k) cudaEventDestroy(ev[k]);
   cudaStreamDestroy(stream);
 }
@@ -246,23 +251,20 @@ int Engine::add_grid(int n_e, const double* E) {
   return (int)grids.size() - 1;
 }
 
-// Per-energy split of t_E = log10(E) (n_E - 1)/(logEkT_max - logEkT_min) for the loaded NSX axis.
-void Engine::prepare_grid(int id) {
-  Grid& g = grids[id];
-  if (!has_nsx) return;
-  if (g.nsx_version == nsx_version) return;
-  const int n = (int)g.E.size();
-  std::vector<int> iE(n), rE(n);
-  std::vector<float> fE(n);
+void split_grid(const std::vector<double>& E, double inv_dE, GridSplit& o) {
+  const int n = (int)E.size();
+  std::vector<int> iE(n);
+  o.rE.assign(n, 0);
+  o.fE.assign(n, 0.0f);
   double lo = 1e300, hi = -1e300;
   int imin = 1 << 30, imax = -(1 << 30);
   for (int i = 0; i < n; ++i) {
-    double t = std::log10(g.E[i]) * nsx.inv_dE;
+    double t = std::log10(E[i]) * inv_dE;
     double fl = std::floor(t);
     iE[i] = (int)fl;
-    fE[i] = (float)(t - fl);
-    if (fE[i] >= 1.0f) {  // rounding of the fraction up to 1
-      fE[i] = 0.0f;
+    o.fE[i] = (float)(t - fl);
+    if (o.fE[i] >= 1.0f) {  // rounding of the fraction up to 1
+      o.fE[i] = 0.0f;
       iE[i] += 1;
     }
     lo = std::min(lo, t);
@@ -270,15 +272,48 @@ void Engine::prepare_grid(int id) {
     imin = std::min(imin, iE[i]);
     imax = std::max(imax, iE[i]);
   }
-  for (int i = 0; i < n; ++i) rE[i] = iE[i] - imin;
-  if (g.drE) cudaFree(g.drE);
-  if (g.dfE) cudaFree(g.dfE);
-  g.drE = dev_upload(rE.data(), n);
-  g.dfE = dev_upload(fE.data(), n);
-  g.iE_min = imin;
-  g.span = imax - imin + 1;
-  g.tE_lo = lo;
-  g.tE_hi = hi;
+  for (int i = 0; i < n; ++i) o.rE[i] = iE[i] - imin;
+  o.iE_min = imin;
+  o.span = imax - imin + 1;
+  o.lo = lo;
+  o.hi = hi;
+  // energies grouped by home cell, ascending fraction inside a cell
+  o.perm.resize(n);
+  for (int i = 0; i < n; ++i) o.perm[i] = i;
+  std::stable_sort(o.perm.begin(), o.perm.end(), [&](int a, int b) {
+    return o.rE[a] != o.rE[b] ? o.rE[a] < o.rE[b] : o.fE[a] < o.fE[b];
+  });
+  o.fEs.resize(n);
+  for (int i = 0; i < n; ++i) o.fEs[i] = o.fE[o.perm[i]];
+  o.cell_first.assign(o.span + 1, 0);
+  for (int i = 0; i < n; ++i) o.cell_first[o.rE[i] + 1] += 1;
+  o.maxe = 0;
+  for (int r = 0; r < o.span; ++r) {
+    o.maxe = std::max(o.maxe, o.cell_first[r + 1]);
+    o.cell_first[r + 1] += o.cell_first[r];
+  }
+}
+
+// Per-energy split of t_E = log10(E) (n_E - 1)/(logEkT_max - logEkT_min) for the loaded NSX axis.
+void Engine::prepare_grid(int id) {
+  Grid& g = grids[id];
+  if (!has_nsx) return;
+  if (g.nsx_version == nsx_version) return;
+  GridSplit sp;
+  split_grid(g.E, nsx.inv_dE, sp);
+  const int n = (int)g.E.size();
+  for (void* q : {(void*)g.drE, (void*)g.dfE, (void*)g.dperm, (void*)g.dfEs, (void*)g.dcell_first})
+    if (q) cudaFree(q);
+  g.drE = dev_upload(sp.rE.data(), n);
+  g.dfE = dev_upload(sp.fE.data(), n);
+  g.dperm = dev_upload(sp.perm.data(), n);
+  g.dfEs = dev_upload(sp.fEs.data(), n);
+  g.dcell_first = dev_upload(sp.cell_first.data(), sp.cell_first.size());
+  g.maxe = sp.maxe;
+  g.iE_min = sp.iE_min;
+  g.span = sp.span;
+  g.tE_lo = sp.lo;
+  g.tE_hi = sp.hi;
   g.nsx_version = nsx_version;
 }
 
@@ -294,6 +329,10 @@ DevGrid Engine::dev_grid(int id) {
   d.invE = g.dinvE;
   d.rE = g.drE;
   d.fE = g.dfE;
+  d.perm = g.dperm;
+  d.fEs = g.dfEs;
+  d.cell_first = g.dcell_first;
+  d.maxe = g.maxe;
   return d;
 }
 
@@ -619,17 +658,19 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
     q.next = B.d_ctrl + 3 * v + 1;
     q.overflow = B.d_ctrl + 3 * v + 2;
     base += cap[v];
-    int ne_max = 1, nf_max = 2, cells_max = 2;
+    int ne_max = 1, nf_max = 2, cells_max = 2, maxe_max = 0, bins_max = 0;
     for (int k = g0; k < g1; ++k) {
       ne_max = std::max(ne_max, hp[k].n_e);
       nf_max = std::max(nf_max, hp[k].n_fine);
       cells_max = std::max(cells_max, hp[k].grid.span + 1);
+      maxe_max = std::max(maxe_max, hp[k].grid.maxe);
+      bins_max = std::max(bins_max, hp[k].n_bins);
     }
     G.args.profiles = B.d_prof + g0;
     G.args.lens = lens;
     G.args.nsx = nsx;
     G.args.flux = B.d_flux;
-    G.args.shape = choose_shape(v == 0, v == 1, ne_max, nf_max, cells_max);
+    G.args.shape = choose_shape(v == 0, v == 1, ne_max, nf_max, cells_max, maxe_max, bins_max);
     PPM_CUDA(configure_integrand_smem(G.args.shape));
     const int occ = max_active_ctas(G.args.shape);
     if (occ < 1)
@@ -788,7 +829,28 @@ void Engine::profile_batch(int n, const ppm_params* ps, double* flux, double* co
   batch_collect(B, flux, counts, info, stream);
 }
 
-IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max) {
+IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max, int maxe_max,
+                                    int bins_max) {
+  // home-cell NSX kernel: one warp per 28 cells of a point, warp sets up to 512 threads
+  const int span_max = cells_max - 1;
+  const int cell_warps = (span_max + kCellsPerWarp - 1) / kCellsPerWarp;
+  if (nsx_kernel && tune.kernel == 0 && maxe_max >= 1 && maxe_max <= 16 && cell_warps <= 16 && nsx.nmu < 4096 &&
+      bins_max < (1 << 20)) {
+    // default: 256 threads (three CTAs of 80 registers per SM measured fastest)
+    int sets = std::min(16 / cell_warps, tune.sets > 0 ? tune.sets : std::max(1, 8 / cell_warps));
+    IntegrandShape s;
+    for (;;) {
+      const int nt = 32 * cell_warps * sets;
+      s = make_shape(true, nt, 1, 1, tune.chunk, nf_max, lens.n_cp, lens.n_ca, nsx.nE, nsx.nmu, cells_max, true);
+      if (s.total <= 200 * 1024 || sets == 1) break;
+      --sets;
+    }
+    s.bb_fp64 = 0;
+    s.cell_warps = cell_warps;
+    s.maxe_t = maxe_max <= 4 ? 4 : (maxe_max <= 8 ? 8 : 16);
+    s.minb = s.maxe_t <= 8 ? tune.minb : 1;
+    return s;
+  }
   int ne_t = 1;
   if (ne_max > 512)
     ne_t = 4;
@@ -808,7 +870,7 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
     pb -= nwarps;
   }
   s.bb_fp64 = bb_fp64 ? 1 : 0;
-  s.minb = (ne_t <= 2 && nt <= 320) ? tune.minb : 1;
+  s.minb = (ne_t <= 2 && nt <= 320) ? std::min(tune.minb, 2) : 1;
   return s;
 }
 
@@ -833,8 +895,8 @@ std::string Engine::autotune(int n, const ppm_params* sample) {
   std::string rep;
   auto line = [&](const Tuning& t, float ms, const char* note) {
     char buf[160];
-    std::snprintf(buf, sizeof(buf), "pb=%d chunk=%d minb=%d ne_t=%d : %.3f ms%s\n", t.pb, t.chunk, t.minb, t.ne_t, ms,
-                  note);
+    std::snprintf(buf, sizeof(buf), "pb=%d chunk=%d minb=%d ne_t=%d sets=%d kernel=%d : %.3f ms%s\n", t.pb, t.chunk,
+                  t.minb, t.ne_t, t.sets, t.kernel, ms, note);
     rep += buf;
   };
   Tuning best = start;
@@ -843,8 +905,10 @@ std::string Engine::autotune(int n, const ppm_params* sample) {
   const std::vector<std::pair<int Tuning::*, std::vector<int>>> dims = {
       {&Tuning::pb, {10, 20, 30, 40}},
       {&Tuning::chunk, {256, 512, 1024, 2048}},
-      {&Tuning::minb, {1, 2}},
+      {&Tuning::minb, {1, 2, 3}},
       {&Tuning::ne_t, {0, 2}},
+      {&Tuning::sets, {0, 1, 2, 3, 4}},
+      {&Tuning::kernel, {0, 1}},
   };
   for (const auto& d : dims) {
     for (int v : d.second) {

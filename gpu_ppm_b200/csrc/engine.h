@@ -49,6 +49,10 @@ struct Grid {
   double* dinvE = nullptr;
   int* drE = nullptr;
   float* dfE = nullptr;
+  int* dperm = nullptr;
+  float* dfEs = nullptr;
+  int* dcell_first = nullptr;
+  int maxe = 0;
   int iE_min = 0, span = 1;
   double tE_lo = 0, tE_hi = 0;
   int nsx_version = -1;
@@ -107,11 +111,23 @@ struct BatchImpl {
   ~BatchImpl();
 };
 
+// Split of an energy grid against the NSX logEkT axis: t_E = log10(E) inv_dE =
+// iE_min + rE + fE, plus the energies grouped by home cell rE in t_E order.
+struct GridSplit {
+  std::vector<int> rE, perm, cell_first;
+  std::vector<float> fE, fEs;
+  int iE_min = 0, span = 1, maxe = 0;
+  double lo = 0, hi = 0;
+};
+void split_grid(const std::vector<double>& E, double inv_dE, GridSplit& out);
+
 struct Tuning {
   int pb = 20;       // phase points per polynomial sub-batch (rounded to whole warps)
   int chunk = 1024;  // candidate elements per tile
   int ne_t = 0;      // energies per thread (0 = automatic)
-  int minb = 2;      // CTAs per SM targeted by the register budget
+  int minb = 2;      // CTAs per SM targeted by the register budget (3: home-cell kernel with <= 256 threads only)
+  int kernel = 0;    // NSX integrand: 0 = home-cell kernel where the grid allows, 1 = pooled-polynomial kernel
+  int sets = 0;      // home-cell kernel: warp sets per CTA (0 = 256 threads)
 };
 
 struct GraphEntry {
@@ -167,7 +183,8 @@ class Engine {
   DevGrid dev_grid(int id);
   const double* ring_table(int N);
   const double* fine_table(int nf);
-  IntegrandShape choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max);
+  IntegrandShape choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max, int maxe_max = 0,
+                              int bins_max = 0);
   void fold_tc_prepare(Resp& r);
   cudaError_t fold_tc_launch(const Resp& r, const FoldJob* jobs, int n_jobs, int n_bins, const double* flux,
                              double* counts, cudaStream_t st);

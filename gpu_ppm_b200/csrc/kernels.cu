@@ -514,6 +514,316 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 320, MINB) integrand_nsx_ker
 }
 
 // ---------------------------------------------------------------------------
+// Home-cell NSX integrand.
+//
+// For a phase point with cell origin G0 and cell fraction fP, energy e falls
+// in NSX cell G0 + rE[e] + carry (carry = fE[e] + fP >= 1).  Every lane owns
+// one home cell r = rE (28 per warp) and the few energies whose rE is r, so
+// per point it needs the cubic polynomials of cells G0 + r and G0 + r + 1,
+// i.e. the mu-contracted slice H at G0 + r - 1 .. G0 + r + 3: each lane
+// contracts one row of the slice (H at G0 + r - 1) and takes the next four
+// from its neighbours by warp shuffles (lanes 28..31 only supply them).
+// Polynomials and partial sums stay in registers; a warp set of cell_warps
+// warps covers every cell of a point, and the CTA's warp sets take the
+// point records in contiguous runs, each keeping its own per-bin partial sums.
+//
+// The polynomial of a cell is the one the pooled kernel builds (4-point
+// Lagrange stencil clamped at the table ends, cpu/nsx.hpp:187-225, written
+// as Newton differences in the cell fraction); outside the logEkT axis the
+// edge value is held (cpu/hunt.hpp:98-121 clamps the coordinate).
+__device__ __forceinline__ float slice_dot(const float* S, int ldS, int k, int imu, float4 w) {
+  const float* row = S + k * ldS + imu;
+  return fmaf(w.w, row[3], fmaf(w.z, row[2], fmaf(w.y, row[1], w.x * row[0])));
+}
+
+// cubic through h0..h3 at stencil nodes 0..3, in the fraction of cell `off` (0, 1, 2)
+__device__ __forceinline__ float4 cubic_cell(float h0, float h1, float h2, float h3, int off) {
+  const float d1 = h1 - h0, d2 = h2 - 2.f * h1 + h0, d3 = h3 - 3.f * h2 + 3.f * h1 - h0;
+  const float c3 = d3 * (1.f / 6.f);
+  if (off == 1) return make_float4(h1, d1 + 0.5f * d2 - c3, 0.5f * d2, c3);
+  if (off == 0) return make_float4(h0, d1 - 0.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 - 0.5f * d3, c3);
+  return make_float4(h2, d1 + 1.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 + 0.5f * d3, c3);
+}
+
+// Polynomials of cells G0 + r and G0 + r + 1 for one point record; called by
+// the whole warp (shuffles).  rec = {c, fP, bin | imu << 20, G0}, w = mu weights.
+// Sx points at slice row 0 of a slice with two extra rows: row -1 and row nE
+// hold the cubic extrapolations of the first and last four rows, so that the
+// centred stencil of cell 0 (rows -1..2) and of cell nE - 2 (rows nE - 3..nE)
+// is the same cubic as the end-clamped stencil (rows 0..3, rows nE - 4..nE - 1).
+// Each lane contracts row r(G0 + r - 1) with r(k) = 0 for k < -1 and nE - 1
+// for k > nE, so cells past either end see the end value H[0] / H[nE - 1].
+__device__ __forceinline__ void cell_polys(const float* Sx, int ldS, int nE, int r, bool cubicE, float4 rec, float4 w,
+                                           float4& Q0, float4& Q1) {
+  const int imu = (int)(__float_as_uint(rec.z) >> 20);
+  const int g = __float_as_int(rec.w) + r;
+  const int k = g - 1;
+  const int row = k < -1 ? 0 : (k > nE ? nE - 1 : k);
+  const float h0 = slice_dot(Sx, ldS, row, imu, w);
+  const float h1 = __shfl_down_sync(0xffffffffu, h0, 1);
+  const float h2 = __shfl_down_sync(0xffffffffu, h0, 2);
+  const float h3 = __shfl_down_sync(0xffffffffu, h0, 3);
+  const float h4 = __shfl_down_sync(0xffffffffu, h0, 4);
+  if (cubicE) {
+    Q0 = cubic_cell(h0, h1, h2, h3, 1);
+    Q1 = cubic_cell(h1, h2, h3, h4, 1);
+  } else {
+    Q0 = make_float4(h1, h2 - h1, 0.f, 0.f);
+    Q1 = make_float4(h2, h3 - h2, 0.f, 0.f);
+  }
+  // cells past an end hold the end value: H[0] is h0 there; H[nE - 1] is h1,
+  // except where the lane's neighbour holds the extrapolated row nE
+  if (g < 0) Q0 = make_float4(h0, 0.f, 0.f, 0.f);
+  if (g > nE - 2) Q0 = make_float4(g == nE ? h0 : h1, 0.f, 0.f, 0.f);
+  if (g < -1) Q1 = make_float4(h0, 0.f, 0.f, 0.f);
+  if (g > nE - 3) Q1 = make_float4(g == nE - 1 ? h1 : h2, 0.f, 0.f, 0.f);
+}
+
+// value at split coordinate t = fE + fP in [0, 2): cell Q0 below 1, Q1 (carry) above
+__device__ __forceinline__ float cell_eval(const float4& Q0, const float4& Q1, float t, bool sg) {
+  const bool carry = t >= 1.f;
+  t = carry ? t - 1.f : t;
+  const float4 q = carry ? Q1 : Q0;
+  float v = fmaf(fmaf(fmaf(q.w, t, q.z), t, q.y), t, q.x);
+  return sg ? fmaxf(v, 0.f) : v;
+}
+
+template <int MAXE, int NTMAX, int MINB>
+__global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const KernelArgs a) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  const IntegrandShape& S = a.shape;
+  const SmemPtrs s = carve(sm, S);
+  __shared__ RingGeom s_g;
+  __shared__ int s_int[48];
+  __shared__ int s_tile;
+  __shared__ float s_tapw[16];
+  __shared__ int s_tapo[16];
+  __shared__ int s_ntap;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const DevNsx& X = a.nsx;
+  const int nE = X.nE, nmu = X.nmu, ldS = S.ldS;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int set = warp / S.cell_warps, n_sets = (nt >> 5) / S.cell_warps;
+  const int r = (warp - set * S.cell_warps) * kCellsPerWarp + lane;  // home cell (lanes 28..31: halo only)
+  float4* rec = (float4*)s.batch;  // [nt][2]: {c, fP, bin | imu << 20, G0}, {mu weights}
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_tile = atomicAdd(a.queue.next, 1);
+    __syncthreads();
+    const int t = s_tile;
+    if (t >= *a.queue.n_tiles || t >= a.queue.capacity) break;
+    const Tile tile = a.queue.tiles[t];
+    const DevProfile& p = a.profiles[tile.profile];
+    const DevSpot& sp = p.spot[tile.spot];
+    const bool point = sp.kind == 1;
+    const int n_act = tile_prologue(a, p, sp, tile, s, s_g, s_int, true);
+    if (n_act == 0) continue;
+
+    // ---- (logT, logg) pre-reduction of the NSX table into S[E][mu] (row stride ldS)
+    if (tid == 0) {
+      const bool cubic = (p.interp == 0 || p.interp == 1 || p.interp == 2);
+      double lg = s_g.logg, ag;
+      s_int[45] = (lg < X.g_min || lg > X.g_max) ? 1 : 0;
+      s_int[44] = 0;
+      int ig = uhunt(lg, X.g_min, X.g_max, X.ng, ag);
+      double wg[4];
+      int ig0, ngt;
+      if (cubic) {
+        ig0 = clampi(ig - 1, 0, X.ng - 4);
+        cubic_lagrange(wg, lg, uhunt_at(X.g_min, X.g_max, X.ng, ig0), uhunt_at(X.g_min, X.g_max, X.ng, ig0 + 1),
+                       uhunt_at(X.g_min, X.g_max, X.ng, ig0 + 2), uhunt_at(X.g_min, X.g_max, X.ng, ig0 + 3));
+        ngt = 4;
+      } else {
+        ig0 = ig;
+        wg[0] = 1 - ag;
+        wg[1] = ag;
+        ngt = 2;
+      }
+      int n = 0;
+      for (int jt = 0; jt < sp.nT_taps; ++jt)
+        for (int jg = 0; jg < ngt; ++jg) {
+          s_tapw[n] = (float)(sp.wT[jt] * wg[jg]);
+          s_tapo[n] = (sp.iT[jt] * X.ng + ig0 + jg) * X.slice_stride;
+          ++n;
+        }
+      s_ntap = n;
+    }
+    for (int k = tid; k < nmu; k += nt) s.mu[k] = X.mu[k];
+    for (int k = tid; k < 4 * (nmu - 3); k += nt) s.mu[nmu + k] = X.mu_den[k];
+    __syncthreads();
+    // slice rows 0..nE-1 start 16-byte aligned after room for row -1; row nE follows them
+    float* const Sx = s.S + ((ldS + 3) & ~3);
+    {
+      const int ntap = s_ntap, n_el = nE * nmu;
+      if (ldS == nmu) {
+        const int n4 = (n_el + 3) >> 2;
+        float4* S4 = (float4*)Sx;
+        for (int k = tid; k < n4; k += nt) {
+          float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+          for (int q = 0; q < ntap; ++q) {
+            const float4 v = __ldg((const float4*)(X.data + s_tapo[q]) + k);
+            const float w = s_tapw[q];
+            acc.x = fmaf(w, v.x, acc.x);
+            acc.y = fmaf(w, v.y, acc.y);
+            acc.z = fmaf(w, v.z, acc.z);
+            acc.w = fmaf(w, v.w, acc.w);
+          }
+          S4[k] = acc;
+        }
+      } else {
+        for (int k = tid; k < n_el; k += nt) {
+          float acc = 0.f;
+          for (int q = 0; q < ntap; ++q) acc = fmaf(s_tapw[q], __ldg(X.data + s_tapo[q] + k), acc);
+          const int row = k / nmu;
+          Sx[row * ldS + (k - row * nmu)] = acc;
+        }
+      }
+    }
+    __syncthreads();
+    // rows -1 and nE: the cubic through the first (last) four rows, one row further out
+    for (int k = tid; k < 2 * nmu; k += nt) {
+      const int top = k >= nmu, m = top ? k - nmu : k;
+      const float* a = Sx + (top ? (nE - 1) * ldS : 0) + m;
+      const int st = top ? -ldS : ldS;
+      Sx[(top ? nE : -1) * ldS + m] = fmaf(4.f, a[0], fmaf(-6.f, a[st], fmaf(4.f, a[2 * st], -a[3 * st])));
+    }
+    __syncthreads();
+
+    // ---- deposit
+    const DevGrid& G = p.grid;
+    const int n_e = G.n_e;
+    int e0 = 0, cnt = 0;
+    if (lane < kCellsPerWarp && r < G.span) {
+      e0 = G.cell_first[r];
+      cnt = min(G.cell_first[r + 1] - e0, MAXE);
+    }
+    float fE[MAXE], acc[MAXE];
+#pragma unroll
+    for (int k = 0; k < MAXE; ++k) {
+      fE[k] = k < cnt ? G.fEs[e0 + k] : 0.f;
+      acc[k] = 0.f;
+    }
+    const int mode = p.interp;
+    const bool cubicE = mode != 4;
+    const bool sg = mode == 1;
+    const double mu_min = s.mu[nmu - 1];
+    const int n_pp = p.n_gl > 0 ? p.n_bins * p.n_gl : p.n_bins;
+    const int n_pts = n_pp * n_act;
+    int cur_bin = -1;
+    double* flux_base = a.flux + p.flux_off;
+    const double out_scale = sp.out_scale;
+
+    auto flush = [&]() {
+#pragma unroll
+      for (int k = 0; k < MAXE; ++k) {
+        if (k < cnt && acc[k] != 0.f) {
+          const int e = G.perm[e0 + k];
+          atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)acc[k] * out_scale * G.invE[e]);
+        }
+        acc[k] = 0.f;
+      }
+    };
+
+    const double* den = s.mu + nmu;  // [nmu - 3][4] reciprocal Lagrange denominators
+    for (int q0 = 0; q0 < n_pts; q0 += nt) {
+      // every thread evaluates one phase point (FP64); visible ones are
+      // compacted, in order, into the point records
+      bool vis = false, clamped = false;
+      float c = 0.f, fP = 0.f;
+      int G0 = 0, bin = 0, imu = 0;
+      float w4[4] = {0.f, 0.f, 0.f, 0.f};
+      const int q = q0 + tid;
+      if (q < n_pts) {
+        double wgl, z = 0, mu = 0;
+        const double flux = phase_point(p, s, tile.ring, point, n_act, q, bin, wgl, z, mu);
+        if (flux != 0.0) {
+          vis = true;
+          if (mu < mu_min) mu = mu_min;
+          c = (float)(flux * wgl);
+          const double tP = (log10(z) - sp.l10kT - X.E_min) * X.inv_dE;
+          const double fl = floor(tP);
+          fP = (float)(tP - fl);
+          if (fP >= 1.f) fP = 0.99999994f;
+          G0 = G.iE_min + (int)fl;
+          clamped = (G.tE_lo + tP < 0.0) || (G.tE_hi + tP > (double)(nE - 1)) || sp.T_clamped || s_int[45];
+          // mu weights (cpu/nsx.hpp:173-321)
+          double am;
+          const int im = vhunt(s.mu, nmu, mu, am);
+          const bool linear_mu = (mode == 4) || ((mode == 2 || mode == 3) && im >= nmu - 5);
+          int start;
+          if (linear_mu) {
+            start = min(im, nmu - 4);
+            const int o = im - start;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) w4[k] = k == o ? (float)(1 - am) : (k == o + 1 ? (float)am : 0.f);
+          } else {
+            start = clampi(im - 1, 0, nmu - 4);
+            const double x0 = s.mu[start], x1 = s.mu[start + 1], x2 = s.mu[start + 2], x3 = s.mu[start + 3];
+            const double* rd = den + 4 * start;
+            w4[0] = (float)((mu - x1) * (mu - x2) * (mu - x3) * rd[0]);
+            w4[1] = (float)((mu - x0) * (mu - x2) * (mu - x3) * rd[1]);
+            w4[2] = (float)((mu - x0) * (mu - x1) * (mu - x3) * rd[2]);
+            w4[3] = (float)((mu - x0) * (mu - x1) * (mu - x2) * rd[3]);
+          }
+          imu = start;
+        }
+      }
+      int nv;
+      const int slot = block_compact(vis, s_int, &nv);
+      if (vis) {
+        rec[2 * slot] = make_float4(c, fP, __uint_as_float((unsigned)bin | ((unsigned)imu << 20)), __int_as_float(G0));
+        rec[2 * slot + 1] = make_float4(w4[0], w4[1], w4[2], w4[3]);
+        if (clamped) atomicAdd(&s_int[44], 1);
+      }
+      __syncthreads();
+      if (tid == 0) {
+        if (nv) atomicAdd(&p.stats[3], (unsigned long long)nv);
+        if (s_int[44]) atomicAdd(&p.stats[4], (unsigned long long)s_int[44]);
+        s_int[44] = 0;
+      }
+
+      // each warp set takes a contiguous run of the records (one flush per bin
+      // change in its run); two records of the same bin are interleaved
+      const int b_end = (int)((long long)nv * (set + 1) / n_sets);
+      for (int b = (int)((long long)nv * set / n_sets); b < b_end;) {
+        const float4 rA = rec[2 * b], wA = rec[2 * b + 1];
+        const int binA = (int)(__float_as_uint(rA.z) & 0xFFFFFu);
+        if (binA != cur_bin) {
+          if (cur_bin >= 0) flush();
+          cur_bin = binA;
+        }
+        bool two = false;
+        float4 rB = rA, wB = wA;
+        if (b + 1 < b_end) {
+          rB = rec[2 * b + 2];
+          wB = rec[2 * b + 3];
+          two = (int)(__float_as_uint(rB.z) & 0xFFFFFu) == binA;
+        }
+        float4 A0, A1;
+        cell_polys(Sx, ldS, nE, r, cubicE, rA, wA, A0, A1);
+        if (two) {
+          float4 B0, B1;
+          cell_polys(Sx, ldS, nE, r, cubicE, rB, wB, B0, B1);
+#pragma unroll
+          for (int k = 0; k < MAXE; ++k) {
+            const float va = cell_eval(A0, A1, fE[k] + rA.y, sg), vb = cell_eval(B0, B1, fE[k] + rB.y, sg);
+            acc[k] = fmaf(rB.x, vb, fmaf(rA.x, va, acc[k]));
+          }
+          b += 2;
+        } else {
+#pragma unroll
+          for (int k = 0; k < MAXE; ++k) acc[k] = fmaf(rA.x, cell_eval(A0, A1, fE[k] + rA.y, sg), acc[k]);
+          b += 1;
+        }
+      }
+      __syncthreads();
+    }
+    if (cur_bin >= 0) flush();
+  }
+}
+
+// ---------------------------------------------------------------------------
 template <typename Real, int NE_T>
 __global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
@@ -766,9 +1076,10 @@ __global__ void fold_simt_kernel(const FoldJob* jobs, const double* rsp, int n_c
 
 // ---------------------------------------------------------------------------
 IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int n_fine, int n_cp, int n_ca, int nE,
-                          int nmu, int cells) {
+                          int nmu, int cells, bool cellk) {
   IntegrandShape s{};
   s.nsx = nsx;
+  s.cellk = (nsx && cellk) ? 1 : 0;
   s.nt = nt;
   s.ne_t = ne_t;
   s.pb = pb;
@@ -795,11 +1106,27 @@ IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int 
   s.off_mu = off;
   off += nsx ? al((long)nmu * 8 * 5) : 0;
   s.off_S = off;
+  const int rows = al((long)(4 * n_cp + 2 * n_ca) * 8);
+  if (s.cellk) {
+    // home-cell kernel: odd row stride; the lensing rows (used only by the
+    // sweep, before the slice is built) share the slice's space; 32-byte point records
+    s.ldS = nmu | 1;
+    // rows -1 .. nE, row 0 16-byte aligned
+    const int slice = al(((long)((s.ldS + 3) & ~3) + (long)(nE + 1) * s.ldS) * 4);
+    s.off_rows = off;
+    off += slice > rows ? slice : rows;
+    s.off_union = off;
+    s.off_batch = off;
+    s.off_Q = off;
+    off += al((long)nt * 32);
+    s.total = off;
+    return s;
+  }
+  s.ldS = nmu;
   // the slice is stored with the table's 16-byte aligned stride
   const long slice = nsx ? ((long)nE * nmu + 3) / 4 * 4 : 0;
   off += al(slice * 4);
   s.off_union = off;
-  const int rows = al((long)(4 * n_cp + 2 * n_ca) * 8);
   const int batch = al((long)nt * kSlotBytes);
   const int qbuf = nsx ? al((long)pb * cells * 16) + al((long)pb * (cells + 3) * 4) : 0;
   s.off_rows = off;
@@ -812,6 +1139,21 @@ IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int 
 
 namespace {
 void* kernel_for(const IntegrandShape& s, int precision) {
+  if (s.nsx && s.cellk) {
+    // register budget: CTAs per SM (minb) at the launch's thread count
+    const int v = s.minb >= 3 && s.nt <= 256 ? 3 : (s.minb >= 2 ? (s.nt <= 384 ? 2 : 1) : 0);
+    if (s.maxe_t == 4) {
+      void* f[] = {(void*)integrand_nsx_cell_kernel<4, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 512, 2>,
+                   (void*)integrand_nsx_cell_kernel<4, 384, 2>, (void*)integrand_nsx_cell_kernel<4, 256, 3>};
+      return f[v];
+    }
+    if (s.maxe_t == 8) {
+      void* f[] = {(void*)integrand_nsx_cell_kernel<8, 512, 1>, (void*)integrand_nsx_cell_kernel<8, 512, 2>,
+                   (void*)integrand_nsx_cell_kernel<8, 384, 2>, (void*)integrand_nsx_cell_kernel<8, 256, 3>};
+      return f[v];
+    }
+    return (void*)integrand_nsx_cell_kernel<16, 512, 1>;
+  }
   if (s.nsx) {
     const bool two = s.minb >= 2;
     switch (s.ne_t) {
@@ -839,7 +1181,12 @@ cudaError_t configure_integrand_smem(const IntegrandShape& s) {
   // all variants get the largest dynamic shared memory allowance once
   static bool done = false;
   if (done) return cudaSuccess;
-  void* fns[] = {(void*)integrand_nsx_kernel<1, 1>, (void*)integrand_nsx_kernel<1, 2>,
+  void* fns[] = {(void*)integrand_nsx_cell_kernel<4, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 512, 2>,
+                 (void*)integrand_nsx_cell_kernel<4, 384, 2>, (void*)integrand_nsx_cell_kernel<4, 256, 3>,
+                 (void*)integrand_nsx_cell_kernel<8, 512, 1>, (void*)integrand_nsx_cell_kernel<8, 512, 2>,
+                 (void*)integrand_nsx_cell_kernel<8, 384, 2>, (void*)integrand_nsx_cell_kernel<8, 256, 3>,
+                 (void*)integrand_nsx_cell_kernel<16, 512, 1>,
+                 (void*)integrand_nsx_kernel<1, 1>, (void*)integrand_nsx_kernel<1, 2>,
                  (void*)integrand_nsx_kernel<2, 1>, (void*)integrand_nsx_kernel<2, 2>, (void*)integrand_nsx_kernel<4, 1>,
                  (void*)integrand_bb_kernel<double, 1>, (void*)integrand_bb_kernel<double, 2>,
                  (void*)integrand_bb_kernel<double, 4>, (void*)integrand_bb_kernel<float, 1>,

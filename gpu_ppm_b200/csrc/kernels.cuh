@@ -21,12 +21,19 @@ struct IntegrandShape {
   bool nsx;
   int bb_fp64;    // blackbody variant: 1 = FP64 integrand, 0 = FP32
   int minb;       // CTAs per SM the register budget is compiled for (1 or 2)
+  // home-cell NSX kernel: one lane per energy cell, record groups of cell_warps warps
+  int cellk;      // 1 = home-cell kernel, 0 = pooled-polynomial kernel
+  int maxe_t;     // energies per lane the home-cell kernel is compiled for (4, 8, 16)
+  int cell_warps; // warps covering the cells of one point (28 cells per warp)
+  int ldS;        // floats between the slice rows in shared memory (odd: conflict-free column reads)
   // offsets in bytes
   int off_j, off_P, off_F, off_Z, off_MU, off_mu, off_S, off_union, off_rows, off_batch, off_Q, total;
 };
 
 IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int n_fine, int n_cp, int n_ca, int nE,
-                          int nmu, int cells);
+                          int nmu, int cells, bool cellk = false);
+// cells a lane of the home-cell kernel owns per warp (4 lanes hold the stencil halo)
+constexpr int kCellsPerWarp = 28;
 
 struct KernelArgs {
   const DevProfile* profiles;

@@ -85,10 +85,19 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   off += up256(sizeof(double) * 3 * 4 * (size_t)N);
   const size_t o_fine = off;
   off += up256(sizeof(double) * 2 * (size_t)nf);
+  GridSplit split;
+  if (nsx_atm) split_grid(gr.E, nsx.inv_dE, split);
+  const size_t n_cf = nsx_atm ? split.cell_first.size() : 1;
   const size_t o_rE = off;
   off += up256(sizeof(int) * (size_t)n_e);
   const size_t o_fE = off;
   off += up256(sizeof(float) * (size_t)n_e);
+  const size_t o_perm = off;
+  off += up256(sizeof(int) * (size_t)n_e);
+  const size_t o_fEs = off;
+  off += up256(sizeof(float) * (size_t)n_e);
+  const size_t o_cf = off;
+  off += up256(sizeof(int) * n_cf);
   const size_t o_tiles = off;
   if (off > kScratchBytes)
     throw Error(PPM_E_RANGE, "ppm_profile_noalloc: N_side " + std::to_string(N) + " / n_fine " + std::to_string(nf) +
@@ -103,35 +112,25 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   g.n_e = n_e;
   g.E = gr.dE;
   g.invE = gr.dinvE;
-  std::vector<int> rE(n_e, 0);
-  std::vector<float> fE(n_e, 0.0f);
   if (nsx_atm) {
     // per-energy split of t_E = log10(E) (n_E - 1)/(logEkT_max - logEkT_min), as prepare_grid
-    std::vector<int> iE(n_e);
-    double lo = 1e300, hi = -1e300;
-    int imin = 1 << 30, imax = -(1 << 30);
-    for (int i = 0; i < n_e; ++i) {
-      double t = std::log10(gr.E[i]) * nsx.inv_dE;
-      double fl = std::floor(t);
-      iE[i] = (int)fl;
-      fE[i] = (float)(t - fl);
-      if (fE[i] >= 1.0f) {
-        fE[i] = 0.0f;
-        iE[i] += 1;
-      }
-      lo = std::min(lo, t);
-      hi = std::max(hi, t);
-      imin = std::min(imin, iE[i]);
-      imax = std::max(imax, iE[i]);
-    }
-    for (int i = 0; i < n_e; ++i) rE[i] = iE[i] - imin;
-    g.iE_min = imin;
-    g.span = imax - imin + 1;
-    g.tE_lo = lo;
-    g.tE_hi = hi;
+    g.iE_min = split.iE_min;
+    g.span = split.span;
+    g.tE_lo = split.lo;
+    g.tE_hi = split.hi;
+    g.maxe = split.maxe;
+  } else {
+    split.rE.assign(n_e, 0);
+    split.fE.assign(n_e, 0.0f);
+    split.perm.assign(n_e, 0);
+    split.fEs.assign(n_e, 0.0f);
+    split.cell_first.assign(1, 0);
   }
   g.rE = (const int*)(base + o_rE);
   g.fE = (const float*)(base + o_fE);
+  g.perm = (const int*)(base + o_perm);
+  g.fEs = (const float*)(base + o_fEs);
+  g.cell_first = (const int*)(base + o_cf);
 
   DevProfile d;
   unsigned long long* stats = (unsigned long long*)(base + o_stats);
@@ -159,8 +158,15 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
      "ring table upload");
   ck(cudaMemcpyAsync(base + o_fine, fine_rows.data(), sizeof(double) * fine_rows.size(), cudaMemcpyHostToDevice, st),
      "fine-phase table upload");
-  ck(cudaMemcpyAsync(base + o_rE, rE.data(), sizeof(int) * n_e, cudaMemcpyHostToDevice, st), "cell index upload");
-  ck(cudaMemcpyAsync(base + o_fE, fE.data(), sizeof(float) * n_e, cudaMemcpyHostToDevice, st), "cell fraction upload");
+  ck(cudaMemcpyAsync(base + o_rE, split.rE.data(), sizeof(int) * n_e, cudaMemcpyHostToDevice, st), "cell index upload");
+  ck(cudaMemcpyAsync(base + o_fE, split.fE.data(), sizeof(float) * n_e, cudaMemcpyHostToDevice, st),
+     "cell fraction upload");
+  ck(cudaMemcpyAsync(base + o_perm, split.perm.data(), sizeof(int) * n_e, cudaMemcpyHostToDevice, st),
+     "cell order upload");
+  ck(cudaMemcpyAsync(base + o_fEs, split.fEs.data(), sizeof(float) * n_e, cudaMemcpyHostToDevice, st),
+     "ordered fraction upload");
+  ck(cudaMemcpyAsync(base + o_cf, split.cell_first.data(), sizeof(int) * n_cf, cudaMemcpyHostToDevice, st),
+     "cell start upload");
   // state that must start at zero: the caller's flux, the counters and the queue control words
   ck(cudaMemsetAsync(flux_d, 0, sizeof(double) * (size_t)p.n_bins * n_e, st), "flux clear");
   ck(cudaMemsetAsync(base + o_stats, 0, sizeof(unsigned long long) * kStats, st), "counter clear");
@@ -179,7 +185,7 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   q.next = ctrl + 1;
   q.overflow = ctrl + 2;
   const bool bb64 = !nsx_atm && p.precision == PPM_PREC_FP64;
-  a.shape = choose_shape(nsx_atm, bb64, n_e, nf, g.span + 1);
+  a.shape = choose_shape(nsx_atm, bb64, n_e, nf, g.span + 1, g.maxe, p.n_bins);
   ck(configure_integrand_smem(a.shape), "shared-memory attribute");
   const int occ = max_active_ctas(a.shape);
   if (occ < 1) throw Error(PPM_E_RANGE, "ppm_profile_noalloc: launch shape does not fit on an SM");

@@ -23,13 +23,14 @@ class Engine:
         cfg = _abi.EngineConfig(device, max_batch, memory_budget, autotune, n_streams)
         h = ctypes.c_void_p()
         check(lib().ppm_engine_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._lib = lib()  # kept for close() at interpreter exit, when module globals are gone
         self.h = h
         self.grids = {}      # id -> energies
         self.responses = {}  # id -> (grid, n_ch)
 
     def close(self):
         if getattr(self, "h", None):
-            lib().ppm_engine_destroy(self.h)
+            self._lib.ppm_engine_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -158,6 +159,7 @@ class Batch:
         self.params = (_abi.Params * self.n)(*plist)
         h = ctypes.c_void_p()
         check(lib().ppm_batch_create(engine.h, self.n, self.params, ctypes.byref(h)))
+        self._lib = lib()
         self.h = h
         f = ctypes.c_void_p()
         c = ctypes.c_void_p()
@@ -179,7 +181,7 @@ class Batch:
 
     def close(self):
         if getattr(self, "h", None):
-            lib().ppm_batch_destroy(self.engine.h, self.h)
+            self._lib.ppm_batch_destroy(self.engine.h, self.h)
             self.h = None
 
     def __del__(self):

@@ -201,3 +201,31 @@ def test_autotune_keeps_parity(eng_v171019):
     f, c, _ = eng_v171019.profile(plist[0])
     ref, _ = eng_v171019.ora.profile(plist[0], E)
     assert max_rel(f, ref) < TOL32
+
+
+@pytest.mark.parametrize("kernel", ["0", "1"])
+def test_table_edges_and_even_mu(monkeypatch, kernel):
+    """Narrow logEkT axes put energies with large flux beyond the low end
+    (0.6..1.4) or the high end (-0.3..0.5) of the table, where the edge value is
+    held, and an even mu count exercises the padded slice rows; every
+    interpolator, a log-spaced grid (home-cell kernel unless PPM_KERNEL=1) and a
+    dense linear grid (pooled kernel), against the oracle."""
+    monkeypatch.setenv("PPM_KERNEL", kernel)
+    lens = synth.lensing("std")
+    grids = (synth.energy_grid(200, 0.1, 20.0), np.linspace(0.1, 20.0, 700))
+    for axis in ((0.6, 1.4), (-0.3, 0.5)):
+        nsx = synth.nsx("v171019", seed=1, n_mu=66, dims={"n_logEkT": 41, "logEkT": axis})
+        e = Engine()
+        e.load_lensing(lens)
+        e.load_nsx(nsx)
+        ora = oracle.Oracle(lens, nsx)
+        for E in grids:
+            g = e.add_energy_grid(E)
+            for interp in range(5):
+                p = synth.config2_params(g, -1, n_side=24, n_bins=16)
+                p.interp = interp
+                flux, _, info = e.profile(p, want_counts=False)
+                ref, oinfo = ora.profile(p, E)
+                assert info.n_points == oinfo.n_points and info.n_clamped > 0
+                assert max_rel(flux, ref) < TOL32, (axis, interp, len(E))
+        e.close()
