@@ -831,13 +831,13 @@ void Engine::profile_batch(int n, const ppm_params* ps, double* flux, double* co
 
 IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max, int maxe_max,
                                     int bins_max) {
-  // home-cell NSX kernel: one warp per 28 cells of a point, warp sets up to 512 threads
+  // home-cell NSX kernel: one warp per 32 cells of a point, warp sets up to 512 threads
   const int span_max = cells_max - 1;
   const int cell_warps = (span_max + kCellsPerWarp - 1) / kCellsPerWarp;
   if (nsx_kernel && tune.kernel == 0 && maxe_max >= 1 && maxe_max <= 16 && cell_warps <= 16 && nsx.nmu < 4096 &&
       bins_max < (1 << 20)) {
-    // default: 256 threads (three CTAs of 80 registers per SM measured fastest)
-    int sets = std::min(16 / cell_warps, tune.sets > 0 ? tune.sets : std::max(1, 8 / cell_warps));
+    // default: about 384 threads (two CTAs of 80 registers per SM measured fastest)
+    int sets = std::min(16 / cell_warps, tune.sets > 0 ? tune.sets : std::max(1, 12 / cell_warps));
     IntegrandShape s;
     for (;;) {
       const int nt = 32 * cell_warps * sets;

@@ -127,7 +127,7 @@ struct Tuning {
   int ne_t = 0;      // energies per thread (0 = automatic)
   int minb = 2;      // CTAs per SM targeted by the register budget (3: home-cell kernel with <= 256 threads only)
   int kernel = 0;    // NSX integrand: 0 = home-cell kernel where the grid allows, 1 = pooled-polynomial kernel
-  int sets = 0;      // home-cell kernel: warp sets per CTA (0 = 256 threads)
+  int sets = 0;      // home-cell kernel: warp sets per CTA (0 = about 384 threads)
 };
 
 struct GraphEntry {

@@ -518,11 +518,11 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 320, MINB) integrand_nsx_ker
 //
 // For a phase point with cell origin G0 and cell fraction fP, energy e falls
 // in NSX cell G0 + rE[e] + carry (carry = fE[e] + fP >= 1).  Every lane owns
-// one home cell r = rE (28 per warp) and the few energies whose rE is r, so
+// one home cell r = rE (32 per warp) and the few energies whose rE is r, so
 // per point it needs the cubic polynomials of cells G0 + r and G0 + r + 1,
 // i.e. the mu-contracted slice H at G0 + r - 1 .. G0 + r + 3: each lane
-// contracts one row of the slice (H at G0 + r - 1) and takes the next four
-// from its neighbours by warp shuffles (lanes 28..31 only supply them).
+// contracts the first and the last of these rows and takes the three between
+// from its neighbours by warp shuffles.
 // Polynomials and partial sums stay in registers; a warp set of cell_warps
 // warps covers every cell of a point, and the CTA's warp sets take the
 // point records in contiguous runs, each keeping its own per-bin partial sums.
@@ -547,23 +547,25 @@ __device__ __forceinline__ float4 cubic_cell(float h0, float h1, float h2, float
 
 // Polynomials of cells G0 + r and G0 + r + 1 for one point record; called by
 // the whole warp (shuffles).  rec = {c, fP, bin | imu << 20, G0}, w = mu weights.
-// Sx points at slice row 0 of a slice with two extra rows: row -1 and row nE
+// Sx points at slice row 0 of a slice with rows -2 .. nE + 1: rows -1 and nE
 // hold the cubic extrapolations of the first and last four rows, so that the
 // centred stencil of cell 0 (rows -1..2) and of cell nE - 2 (rows nE - 3..nE)
-// is the same cubic as the end-clamped stencil (rows 0..3, rows nE - 4..nE - 1).
-// Each lane contracts row r(G0 + r - 1) with r(k) = 0 for k < -1 and nE - 1
-// for k > nE, so cells past either end see the end value H[0] / H[nE - 1].
-__device__ __forceinline__ void cell_polys(const float* Sx, int ldS, int nE, int r, bool cubicE, float4 rec, float4 w,
-                                           float4& Q0, float4& Q1) {
+// is the same cubic as the end-clamped stencil (rows 0..3, rows nE - 4..nE - 1);
+// rows -2 and nE + 1 repeat rows 0 and nE - 1, and window rows are clamped to
+// -2 .. nE + 1, so cells past either end see the end value H[0] / H[nE - 1].
+// Every lane contracts two rows, j = 0 (h0) and j = 4 (h4) of its window
+// G0 + r - 1 + j; row j of lane l is h0 of lane l + j, or h4 of lane
+// l + j - 4 past the end of the warp.
+__device__ __forceinline__ void cell_polys(const float* Sx, int ldS, int nE, int r, int lane, bool cubicE, float4 rec,
+                                           float4 w, float4& Q0, float4& Q1) {
   const int imu = (int)(__float_as_uint(rec.z) >> 20);
   const int g = __float_as_int(rec.w) + r;
-  const int k = g - 1;
-  const int row = k < -1 ? 0 : (k > nE ? nE - 1 : k);
-  const float h0 = slice_dot(Sx, ldS, row, imu, w);
-  const float h1 = __shfl_down_sync(0xffffffffu, h0, 1);
-  const float h2 = __shfl_down_sync(0xffffffffu, h0, 2);
-  const float h3 = __shfl_down_sync(0xffffffffu, h0, 3);
-  const float h4 = __shfl_down_sync(0xffffffffu, h0, 4);
+  const float h0 = slice_dot(Sx, ldS, min(max(g - 1, -2), nE + 1), imu, w);
+  const float h4 = slice_dot(Sx, ldS, min(max(g + 3, -2), nE + 1), imu, w);
+  const float a1 = __shfl_down_sync(0xffffffffu, h0, 1), b1 = __shfl_sync(0xffffffffu, h4, (lane - 3) & 31);
+  const float a2 = __shfl_down_sync(0xffffffffu, h0, 2), b2 = __shfl_sync(0xffffffffu, h4, (lane - 2) & 31);
+  const float a3 = __shfl_down_sync(0xffffffffu, h0, 3), b3 = __shfl_sync(0xffffffffu, h4, (lane - 1) & 31);
+  const float h1 = lane < 31 ? a1 : b1, h2 = lane < 30 ? a2 : b2, h3 = lane < 29 ? a3 : b3;
   if (cubicE) {
     Q0 = cubic_cell(h0, h1, h2, h3, 1);
     Q1 = cubic_cell(h1, h2, h3, h4, 1);
@@ -572,20 +574,34 @@ __device__ __forceinline__ void cell_polys(const float* Sx, int ldS, int nE, int
     Q1 = make_float4(h2, h3 - h2, 0.f, 0.f);
   }
   // cells past an end hold the end value: H[0] is h0 there; H[nE - 1] is h1,
-  // except where the lane's neighbour holds the extrapolated row nE
-  if (g < 0) Q0 = make_float4(h0, 0.f, 0.f, 0.f);
-  if (g > nE - 2) Q0 = make_float4(g == nE ? h0 : h1, 0.f, 0.f, 0.f);
-  if (g < -1) Q1 = make_float4(h0, 0.f, 0.f, 0.f);
-  if (g > nE - 3) Q1 = make_float4(g == nE - 1 ? h1 : h2, 0.f, 0.f, 0.f);
+  // except where window row 1 is the extrapolated row nE
+  if (__any_sync(0xffffffffu, (unsigned)g > (unsigned)(nE - 3))) {
+    if (g < 0) Q0 = make_float4(h0, 0.f, 0.f, 0.f);
+    if (g > nE - 2) Q0 = make_float4(g == nE ? h0 : h1, 0.f, 0.f, 0.f);
+    if (g < -1) Q1 = make_float4(h0, 0.f, 0.f, 0.f);
+    if (g > nE - 3) Q1 = make_float4(g == nE - 1 ? h1 : h2, 0.f, 0.f, 0.f);
+  }
 }
 
-// value at split coordinate t = fE + fP in [0, 2): cell Q0 below 1, Q1 (carry) above
-__device__ __forceinline__ float cell_eval(const float4& Q0, const float4& Q1, float t, bool sg) {
-  const bool carry = t >= 1.f;
-  t = carry ? t - 1.f : t;
-  const float4 q = carry ? Q1 : Q0;
-  float v = fmaf(fmaf(fmaf(q.w, t, q.z), t, q.y), t, q.x);
-  return sg ? fmaxf(v, 0.f) : v;
+// Packed FP32 pairs (fma/add .f32x2): two records' values in one register pair.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pk(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void upk(f32x2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
 }
 
 template <int MAXE, int NTMAX, int MINB>
@@ -604,7 +620,7 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
   const int nE = X.nE, nmu = X.nmu, ldS = S.ldS;
   const int lane = tid & 31, warp = tid >> 5;
   const int set = warp / S.cell_warps, n_sets = (nt >> 5) / S.cell_warps;
-  const int r = (warp - set * S.cell_warps) * kCellsPerWarp + lane;  // home cell (lanes 28..31: halo only)
+  const int r = (warp - set * S.cell_warps) * kCellsPerWarp + lane;  // home cell
   float4* rec = (float4*)s.batch;  // [nt][2]: {c, fP, bin | imu << 20, G0}, {mu weights}
 
   for (;;) {
@@ -652,8 +668,8 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
     for (int k = tid; k < nmu; k += nt) s.mu[k] = X.mu[k];
     for (int k = tid; k < 4 * (nmu - 3); k += nt) s.mu[nmu + k] = X.mu_den[k];
     __syncthreads();
-    // slice rows 0..nE-1 start 16-byte aligned after room for row -1; row nE follows them
-    float* const Sx = s.S + ((ldS + 3) & ~3);
+    // slice rows 0..nE-1 start 16-byte aligned after room for rows -2, -1; rows nE, nE + 1 follow them
+    float* const Sx = s.S + ((2 * ldS + 3) & ~3);
     {
       const int ntap = s_ntap, n_el = nE * nmu;
       if (ldS == nmu) {
@@ -681,12 +697,14 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
       }
     }
     __syncthreads();
-    // rows -1 and nE: the cubic through the first (last) four rows, one row further out
+    // rows -1 and nE: the cubic through the first (last) four rows, one row
+    // further out; rows -2 and nE + 1: copies of rows 0 and nE - 1
     for (int k = tid; k < 2 * nmu; k += nt) {
       const int top = k >= nmu, m = top ? k - nmu : k;
       const float* a = Sx + (top ? (nE - 1) * ldS : 0) + m;
       const int st = top ? -ldS : ldS;
       Sx[(top ? nE : -1) * ldS + m] = fmaf(4.f, a[0], fmaf(-6.f, a[st], fmaf(4.f, a[2 * st], -a[3 * st])));
+      Sx[(top ? nE + 1 : -2) * ldS + m] = a[0];
     }
     __syncthreads();
 
@@ -694,16 +712,20 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
     const DevGrid& G = p.grid;
     const int n_e = G.n_e;
     int e0 = 0, cnt = 0;
-    if (lane < kCellsPerWarp && r < G.span) {
+    if (r < G.span) {
       e0 = G.cell_first[r];
       cnt = min(G.cell_first[r + 1] - e0, MAXE);
     }
-    float fE[MAXE], acc[MAXE];
+    // per energy slot: its fraction in both halves, and partial sums of the
+    // even (low half) and odd (high half) records of a record pair
+    f32x2 fEb[MAXE], acc[MAXE];
 #pragma unroll
     for (int k = 0; k < MAXE; ++k) {
-      fE[k] = k < cnt ? G.fEs[e0 + k] : 0.f;
-      acc[k] = 0.f;
+      const float f = k < cnt ? G.fEs[e0 + k] : 0.f;
+      fEb[k] = pk(f, f);
+      acc[k] = pk(0.f, 0.f);
     }
+    const f32x2 minus1 = pk(-1.f, -1.f);
     const int mode = p.interp;
     const bool cubicE = mode != 4;
     const bool sg = mode == 1;
@@ -717,11 +739,14 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
     auto flush = [&]() {
 #pragma unroll
       for (int k = 0; k < MAXE; ++k) {
-        if (k < cnt && acc[k] != 0.f) {
+        float lo, hi;
+        upk(acc[k], lo, hi);
+        const float v = lo + hi;
+        if (k < cnt && v != 0.f) {
           const int e = G.perm[e0 + k];
-          atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)acc[k] * out_scale * G.invE[e]);
+          atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)v * out_scale * G.invE[e]);
         }
-        acc[k] = 0.f;
+        acc[k] = pk(0.f, 0.f);
       }
     };
 
@@ -784,7 +809,8 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
       }
 
       // each warp set takes a contiguous run of the records (one flush per bin
-      // change in its run); two records of the same bin are interleaved
+      // change in its run) in pairs of same-bin records, the two halves of
+      // packed FP32 pairs; a record without a partner pairs with itself at weight 0
       const int b_end = (int)((long long)nv * (set + 1) / n_sets);
       for (int b = (int)((long long)nv * set / n_sets); b < b_end;) {
         const float4 rA = rec[2 * b], wA = rec[2 * b + 1];
@@ -800,21 +826,36 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
           wB = rec[2 * b + 3];
           two = (int)(__float_as_uint(rB.z) & 0xFFFFFu) == binA;
         }
-        float4 A0, A1;
-        cell_polys(Sx, ldS, nE, r, cubicE, rA, wA, A0, A1);
+        float4 A0, A1, B0, B1;
+        cell_polys(Sx, ldS, nE, r, lane, cubicE, rA, wA, A0, A1);
         if (two) {
-          float4 B0, B1;
-          cell_polys(Sx, ldS, nE, r, cubicE, rB, wB, B0, B1);
-#pragma unroll
-          for (int k = 0; k < MAXE; ++k) {
-            const float va = cell_eval(A0, A1, fE[k] + rA.y, sg), vb = cell_eval(B0, B1, fE[k] + rB.y, sg);
-            acc[k] = fmaf(rB.x, vb, fmaf(rA.x, va, acc[k]));
-          }
-          b += 2;
+          cell_polys(Sx, ldS, nE, r, lane, cubicE, rB, wB, B0, B1);
         } else {
+          B0 = A0;
+          B1 = A1;
+          rB = rA;
+          rB.x = 0.f;
+        }
+        b += two ? 2 : 1;
+        const f32x2 cw = pk(rA.x, rB.x), fP = pk(rA.y, rB.y);
+        const f32x2 p0x = pk(A0.x, B0.x), p0y = pk(A0.y, B0.y), p0z = pk(A0.z, B0.z), p0w = pk(A0.w, B0.w);
+        const f32x2 p1x = pk(A1.x, B1.x), p1y = pk(A1.y, B1.y), p1z = pk(A1.z, B1.z), p1w = pk(A1.w, B1.w);
 #pragma unroll
-          for (int k = 0; k < MAXE; ++k) acc[k] = fmaf(rA.x, cell_eval(A0, A1, fE[k] + rA.y, sg), acc[k]);
-          b += 1;
+        for (int k = 0; k < MAXE; ++k) {
+          // split coordinate t = fE + fP: cell G0 + r below 1, cell G0 + r + 1 at t - 1 above
+          const f32x2 t0 = add2(fEb[k], fP), t1 = add2(t0, minus1);
+          const f32x2 v0 = fma2(fma2(fma2(p0w, t0, p0z), t0, p0y), t0, p0x);
+          const f32x2 v1 = fma2(fma2(fma2(p1w, t1, p1z), t1, p1y), t1, p1x);
+          float ta, tb, a0, b0, a1, b1;
+          upk(t0, ta, tb);
+          upk(v0, a0, b0);
+          upk(v1, a1, b1);
+          float va = ta >= 1.f ? a1 : a0, vb = tb >= 1.f ? b1 : b0;
+          if (sg) {
+            va = fmaxf(va, 0.f);
+            vb = fmaxf(vb, 0.f);
+          }
+          acc[k] = fma2(cw, pk(va, vb), acc[k]);
         }
       }
       __syncthreads();
@@ -1111,8 +1152,8 @@ IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int 
     // home-cell kernel: odd row stride; the lensing rows (used only by the
     // sweep, before the slice is built) share the slice's space; 32-byte point records
     s.ldS = nmu | 1;
-    // rows -1 .. nE, row 0 16-byte aligned
-    const int slice = al(((long)((s.ldS + 3) & ~3) + (long)(nE + 1) * s.ldS) * 4);
+    // rows -2 .. nE + 1, row 0 16-byte aligned
+    const int slice = al(((long)((2 * s.ldS + 3) & ~3) + (long)(nE + 2) * s.ldS) * 4);
     s.off_rows = off;
     off += slice > rows ? slice : rows;
     s.off_union = off;
