@@ -338,6 +338,9 @@ def main():
         if tj.get("evals"):
             traffic = tj["dram_bytes"] * (evals / tj["evals"])
 
+    integrand_kernel = ("integrand_nsx_kernel" if chosen and "kernel=1" in chosen[0]
+                        else "integrand_nsx_cell_kernel")
+
     # ---- e2e: host parameters in, host counts out, through ppm_profile_batch
     arr = (_abi.Params * n)(*plist)
     counts_host = torch.empty(batch.n_counts, dtype=torch.float64, pin_memory=True)
@@ -399,7 +402,7 @@ def main():
             },
             "e2e": {"value": e2e_value, "unit": "profiles/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {
-                "kernel": "integrand_nsx_kernel", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                "kernel": integrand_kernel, "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                 "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
                 "peak_source": f"FP32 SIMT peak at the measured SM clock: {props.multi_processor_count} SMs x 128 "
                                f"lanes x 2 x {sm_mhz:.0f} MHz (MEASURED_PEAKS.json {pk_src}: hbm {pk.get('hbm_gbs')} "
