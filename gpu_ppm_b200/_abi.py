@@ -96,6 +96,13 @@ class ResultInfo(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class Fit(ctypes.Structure):
+    _fields_ = [("chi2", c_double), ("loglike", c_double), ("model_total", c_double), ("n_zero_model", c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class EngineConfig(ctypes.Structure):
     _fields_ = [
         ("device", c_int32), ("max_batch", c_int32), ("memory_budget", c_int64),
@@ -125,6 +132,11 @@ SIGNATURES = {
     "ppm_batch_launch_timed": (c_int32, [c_void_p, c_void_p, c_void_p, POINTER(ctypes.c_float)]),
     "ppm_batch_kernel_count": (c_int32, [c_void_p, c_void_p, POINTER(c_int32)]),
     "ppm_profile_noalloc": (c_int32, [c_void_p, POINTER(Params), c_void_p, c_void_p, c_void_p]),
+    "ppm_batch_create_rings": (c_int32, [c_void_p, c_int32, POINTER(Params), c_int32, c_int32, POINTER(c_void_p)]),
+    "ppm_profile_rings": (c_int32, [c_void_p, POINTER(Params), c_int32, c_int32, DP, DP, POINTER(ResultInfo)]),
+    "ppm_engine_add_observed": (c_int32, [c_void_p, c_int32, c_int32, DP, POINTER(c_int32)]),
+    "ppm_batch_fit": (c_int32, [c_void_p, c_void_p, c_int32, POINTER(Fit), c_void_p]),
+    "ppm_profile_fit": (c_int32, [c_void_p, POINTER(Params), c_int32, POINTER(Fit), POINTER(ResultInfo)]),
     "ppm_engine_autotune": (c_int32, [c_void_p, c_int32, POINTER(Params), c_char_p, c_int32]),
     "ppm_output_sizes": (c_int32, [c_void_p, POINTER(Params), POINTER(c_int64), POINTER(c_int64)]),
     "ppm_submit": (c_int32, [c_void_p, POINTER(Params), DP, DP, POINTER(c_uint64)]),

@@ -11,7 +11,8 @@ OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libppm_b200.so")
 RUN = os.path.join(OUT_DIR, "ppm_run")
 
-SOURCES = ["kernels.cu", "fold_tc.cu", "engine.cu", "noalloc.cu", "capi.cpp", "serve.cpp", "lensgen.cpp", "util.cpp"]
+SOURCES = ["kernels.cu", "fold_tc.cu", "engine.cu", "noalloc.cu", "fit.cu", "capi.cpp", "serve.cpp", "lensgen.cpp",
+           "util.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

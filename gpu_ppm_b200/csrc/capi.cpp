@@ -249,6 +249,30 @@ int ppm_batch_device_outputs(ppm_batch* b, double** flux, int64_t* n_flux, doubl
   });
 }
 
+int ppm_batch_create_rings(ppm_engine* e, int32_t n, const ppm_params* p, int32_t ring_begin, int32_t ring_end,
+                           ppm_batch** out) {
+  return guarded([&] {
+    if (!p || !out) throw Error(PPM_E_INVALID, "null params or output handle");
+    *out = nullptr;
+    ppm::BatchImpl* b = new ppm::BatchImpl();
+    try {
+      eng(e).batch_build(*b, n, p, nullptr, ring_begin, ring_end);
+    } catch (...) {
+      delete b;
+      throw;
+    }
+    *out = reinterpret_cast<ppm_batch*>(b);
+  });
+}
+
+int ppm_profile_rings(ppm_engine* e, const ppm_params* p, int32_t ring_begin, int32_t ring_end, double* flux,
+                      double* counts, ppm_result_info* info) {
+  return guarded([&] {
+    if (!p) throw Error(PPM_E_INVALID, "null params");
+    eng(e).profile_rings(*p, ring_begin, ring_end, flux, counts, info);
+  });
+}
+
 int ppm_batch_collect(ppm_engine* e, ppm_batch* b, double* flux, double* counts, ppm_result_info* info) {
   return guarded([&] {
     if (!b) throw Error(PPM_E_INVALID, "null batch");
@@ -274,6 +298,27 @@ void ppm_batch_destroy(ppm_engine* e, ppm_batch* b) {
   if (!b) return;
   if (e && e->impl) cudaSetDevice(e->impl->cfg.device);
   delete reinterpret_cast<ppm::BatchImpl*>(b);
+}
+
+int ppm_engine_add_observed(ppm_engine* e, int32_t response, int32_t n_bins, const double* counts, int32_t* observed_id) {
+  return guarded([&] {
+    if (!observed_id) throw Error(PPM_E_INVALID, "null output");
+    *observed_id = eng(e).add_observed(response, n_bins, counts);
+  });
+}
+
+int ppm_batch_fit(ppm_engine* e, ppm_batch* b, int32_t observed_id, ppm_fit* out, void* stream) {
+  return guarded([&] {
+    if (!b) throw Error(PPM_E_INVALID, "null batch");
+    eng(e).batch_fit(*reinterpret_cast<ppm::BatchImpl*>(b), observed_id, out, (cudaStream_t)stream);
+  });
+}
+
+int ppm_profile_fit(ppm_engine* e, const ppm_params* p, int32_t observed_id, ppm_fit* out, ppm_result_info* info) {
+  return guarded([&] {
+    if (!p || !out) throw Error(PPM_E_INVALID, "null params or output");
+    eng(e).profile_fit(*p, observed_id, out, info);
+  });
 }
 
 int ppm_profile_noalloc(ppm_engine* e, const ppm_params* p, double* flux_device, double* counts_device, void* stream) {

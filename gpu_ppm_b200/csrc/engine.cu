@@ -585,8 +585,10 @@ void Engine::fill_profile(const ppm_params& p, DevProfile& d, long long flux_off
 // ---- batches ----------------------------------------------------------------------
 // Converts and uploads n profiles, sizes the work queue and output pools, and
 // records the launch shapes; the batch owns all of its device memory.
-void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t copy_stream) {
+void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t copy_stream, int ring_begin,
+                         int ring_end) {
   if (n < 1) throw Error(PPM_E_INVALID, "empty batch");
+  if (ring_begin > ring_end) throw Error(PPM_E_INVALID, "ring window with begin > end");
   if (n > cfg.max_batch) throw Error(PPM_E_RANGE, "batch larger than max_batch");
   PPM_CUDA(cudaSetDevice(cfg.device));
   B.n = n;
@@ -618,11 +620,23 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
   for (int k = 0; k < n; ++k) {
     const int i = order[k];
     to_device(ps[i], hp[k], B.flux_off[i], B.d_stats + (size_t)kStats * i);
+    for (int s = 0; s < ps[i].n_spots; ++s) {  // ring window (a point source is ring 0)
+      DevSpot& sp = hp[k].spot[s];
+      if (sp.kind == PPM_SPOT_POINT) {
+        if (!(ring_begin <= 0 && 0 < ring_end)) {
+          sp.i_lo = 1;
+          sp.i_hi = 0;
+        }
+      } else {
+        sp.i_lo = std::max(sp.i_lo, ring_begin);
+        sp.i_hi = std::min(sp.i_hi, ring_end - 1);
+      }
+    }
     const int v = variant(ps[i]);
     for (int s = 0; s < ps[i].n_spots; ++s) {
       const DevSpot& sp = hp[k].spot[s];
       if (sp.kind == PPM_SPOT_POINT) {
-        cap[v] += 1;
+        cap[v] += sp.i_hi >= sp.i_lo ? 1 : 0;
       } else if (sp.i_hi >= sp.i_lo) {
         const long long rings = sp.i_hi - sp.i_lo + 1;
         cap[v] += rings * (2 + (4ll * ps[i].n_side + chunk - 1) / chunk);
@@ -816,6 +830,17 @@ void Engine::profile(const ppm_params& p, double* flux, double* counts, ppm_resu
   BatchImpl B;
   batch_build(B, 1, &p);
   batch_enqueue(B, stream, nullptr);  // plain form: direct launches, no graph
+  B.last_stream = stream;
+  batch_collect(B, flux, counts, info, stream);
+}
+
+void Engine::profile_rings(const ppm_params& p, int ring_begin, int ring_end, double* flux, double* counts,
+                           ppm_result_info* info) {
+  std::lock_guard<std::mutex> lk(mu);
+  if (counts && p.response < 0) throw Error(PPM_E_INVALID, "counts requested without a response");
+  BatchImpl B;
+  batch_build(B, 1, &p, nullptr, ring_begin, ring_end);
+  batch_enqueue(B, stream, nullptr);
   B.last_stream = stream;
   batch_collect(B, flux, counts, info, stream);
 }

@@ -105,6 +105,8 @@ struct BatchImpl {
   size_t h2d_bytes = 0;
   cudaGraphExec_t graph = nullptr;
   cudaStream_t last_stream = nullptr;
+  long long* d_fit_off = nullptr;  // counts offset per profile (fit statistics)
+  ppm_fit* d_fit = nullptr;
   BatchImpl() = default;
   BatchImpl(const BatchImpl&) = delete;
   BatchImpl& operator=(const BatchImpl&) = delete;
@@ -130,6 +132,13 @@ struct Tuning {
   int sets = 0;      // home-cell kernel: warp sets per CTA (0 = about 384 threads)
 };
 
+// Observed counts [n_ch][n_bins] for fit statistics.
+struct Observed {
+  int resp = -1, n_bins = 0, n_ch = 0;
+  double* d_counts = nullptr;
+  double lgamma_sum = 0;  // sum lgamma(d + 1)
+};
+
 struct GraphEntry {
   cudaGraphExec_t exec = nullptr;
 };
@@ -148,7 +157,9 @@ class Engine {
 
   void profile(const ppm_params& p, double* flux, double* counts, ppm_result_info* info);
   void profile_batch(int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info);
-  void batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t copy_stream = nullptr);
+  // ring_begin/ring_end: only HEALPix rings i in [ring_begin, ring_end) (point sources count as ring 0)
+  void batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t copy_stream = nullptr, int ring_begin = 0,
+                   int ring_end = 1 << 30);
   size_t request_bytes(const ppm_params& p) const;
   void warm_tables(const ppm_params& p);
   void batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events);
@@ -159,6 +170,11 @@ class Engine {
   void batch_launch_timed(BatchImpl& B, cudaStream_t st, float* ms);
   void output_sizes(const ppm_params& p, int64_t* n_flux, int64_t* n_counts) const;
   void profile_noalloc(const ppm_params& p, double* flux_d, double* counts_d, cudaStream_t st);
+  int add_observed(int resp, int n_bins, const double* counts);
+  void batch_fit(BatchImpl& B, int obs, ppm_fit* out, cudaStream_t st);
+  void profile_fit(const ppm_params& p, int obs, ppm_fit* out, ppm_result_info* info);
+  void profile_rings(const ppm_params& p, int ring_begin, int ring_end, double* flux, double* counts,
+                     ppm_result_info* info);
   std::string autotune(int n, const ppm_params* sample);
 
   // serving
@@ -198,6 +214,7 @@ class Engine {
   std::vector<double> nsx_mu;
   std::vector<Grid> grids;
   std::vector<Resp> resps;
+  std::vector<Observed> observed;
   std::map<int, double*> ring_tabs, fine_tabs;
   std::map<int, std::vector<double>> host_rings;
   std::vector<void*> owned;

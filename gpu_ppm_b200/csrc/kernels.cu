@@ -1036,6 +1036,7 @@ __global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const De
   const DevSpot& sp = p.spot[si];
   const bool nsx = p.atmosphere == 0;
   if (sp.kind == 1) {
+    if (sp.i_lo > sp.i_hi) return;  // outside the batch's ring window
     if (threadIdx.x == 0) {
       RingGeom g;
       ring_geometry(p, L, sp.cos_theta_pt, sp.dOmega_pt, false, g);

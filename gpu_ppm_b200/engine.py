@@ -92,6 +92,20 @@ class Engine:
         check(lib().ppm_profile(self.h, ctypes.byref(p), dptr(flux), dptr(counts), ctypes.byref(info)))
         return flux, counts, info
 
+    def add_observed(self, response, n_bins, counts):
+        """Observed counts [n_ch][n_bins] for fit statistics (ppm_engine_add_observed)."""
+        c = np.ascontiguousarray(counts, dtype=np.float64).ravel()
+        oid = ctypes.c_int32()
+        check(lib().ppm_engine_add_observed(self.h, response, n_bins, dptr(c), ctypes.byref(oid)))
+        return oid.value
+
+    def profile_fit(self, p, observed):
+        """One profile's fit statistics only (ppm_profile_fit): (ppm_fit as dict, info)."""
+        out = _abi.Fit()
+        info = _abi.ResultInfo()
+        check(lib().ppm_profile_fit(self.h, ctypes.byref(p), observed, ctypes.byref(out), ctypes.byref(info)))
+        return out.as_dict(), info
+
     def profile_batch(self, plist, want_flux=True, want_counts=None):
         n = len(plist)
         arr = (_abi.Params * n)(*plist)
@@ -123,9 +137,22 @@ class Engine:
         check(lib().ppm_engine_autotune(self.h, n, arr, buf, len(buf)))
         return buf.value.decode()
 
-    def batch(self, plist):
-        """A device-resident batch: planned once, launched any number of times."""
-        return Batch(self, plist)
+    def batch(self, plist, rings=None):
+        """A device-resident batch: planned once, launched any number of times.
+        rings=(begin, end) keeps only HEALPix rings begin <= i < end (ppm_batch_create_rings)."""
+        return Batch(self, plist, rings)
+
+    def profile_rings(self, p, ring_begin, ring_end, want_flux=True, want_counts=None):
+        """One profile restricted to rings [ring_begin, ring_end) (ppm_profile_rings)."""
+        fs, cs = self.sizes(p)
+        if want_counts is None:
+            want_counts = p.response >= 0
+        flux = np.zeros(fs) if want_flux else None
+        counts = np.zeros(cs) if want_counts else None
+        info = _abi.ResultInfo()
+        check(lib().ppm_profile_rings(self.h, ctypes.byref(p), ring_begin, ring_end, dptr(flux), dptr(counts),
+                                      ctypes.byref(info)))
+        return flux, counts, info
 
     # ---- serving
     def submit(self, p, flux, counts):
@@ -153,12 +180,16 @@ class Batch:
     """Wraps ppm_batch: uploads/plans once; `launch(stream)` replays a CUDA graph
     of plan -> integrand -> fold; outputs stay on the device until `collect`."""
 
-    def __init__(self, engine, plist):
+    def __init__(self, engine, plist, rings=None):
         self.engine = engine
         self.n = len(plist)
         self.params = (_abi.Params * self.n)(*plist)
         h = ctypes.c_void_p()
-        check(lib().ppm_batch_create(engine.h, self.n, self.params, ctypes.byref(h)))
+        if rings is None:
+            check(lib().ppm_batch_create(engine.h, self.n, self.params, ctypes.byref(h)))
+        else:
+            check(lib().ppm_batch_create_rings(engine.h, self.n, self.params, int(rings[0]), int(rings[1]),
+                                               ctypes.byref(h)))
         self._lib = lib()
         self.h = h
         f = ctypes.c_void_p()
@@ -171,6 +202,12 @@ class Batch:
 
     def launch(self, stream=0):
         check(lib().ppm_batch_launch(self.engine.h, self.h, ctypes.c_void_p(stream)))
+
+    def fit(self, observed, stream=0):
+        """Fit statistics of every profile after the last launch (ppm_batch_fit): list of dicts."""
+        out = (_abi.Fit * self.n)()
+        check(lib().ppm_batch_fit(self.engine.h, self.h, observed, out, ctypes.c_void_p(stream)))
+        return [f.as_dict() for f in out]
 
     def collect(self, want_flux=False, want_counts=True):
         flux = np.zeros(self.n_flux) if want_flux else None

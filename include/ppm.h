@@ -220,6 +220,17 @@ int ppm_batch_create(ppm_engine* e, int32_t n, const ppm_params* p, ppm_batch** 
 int ppm_batch_launch(ppm_engine* e, ppm_batch* b, void* stream);
 /* Device pointers and sizes (doubles) of the batch's flux and counts pools. */
 int ppm_batch_device_outputs(ppm_batch* b, double** flux, int64_t* n_flux, double** counts, int64_t* n_counts);
+/* Ring-window forms, for splitting one large profile over several GPUs: only
+ * HEALPix rings i with ring_begin <= i < ring_end contribute (rings are
+ * 1 .. 4 N_side - 1; a point-source spot counts as ring 0).  The flux and the
+ * counts are linear in the rings, so the sum of the outputs over a partition of
+ * [0, 4 N_side) is the full profile (one reduce of the counts finishes it).
+ * The reference integrates all rings of a star in one call
+ * (gpu/devarshi24st_gpu.cu:181-427, cpu/devarshi24st_cpu.cpp:86-241). */
+int ppm_batch_create_rings(ppm_engine* e, int32_t n, const ppm_params* p, int32_t ring_begin, int32_t ring_end,
+                           ppm_batch** out);
+int ppm_profile_rings(ppm_engine* e, const ppm_params* p, int32_t ring_begin, int32_t ring_end, double* flux,
+                      double* counts, ppm_result_info* info);
 /* Waits for the last launch and copies the outputs to host memory (either may be NULL). */
 int ppm_batch_collect(ppm_engine* e, ppm_batch* b, double* flux, double* counts, ppm_result_info* info);
 void ppm_batch_destroy(ppm_engine* e, ppm_batch* b);
@@ -253,6 +264,34 @@ int ppm_profile_noalloc(ppm_engine* e, const ppm_params* p, double* flux_device,
  * for every later launch, and writes a one-line-per-candidate report
  * (truncated to report_len; report may be NULL). */
 int ppm_engine_autotune(ppm_engine* e, int32_t n, const ppm_params* sample, char* report, int32_t report_len);
+
+/* ---- fit statistics (sampler likelihood) ------------------------------------ */
+
+/* Goodness of fit of one profile's counts m[ch][bin] against observed counts
+ * d[ch][bin] of the same response and bin count, computed on the device right
+ * after the fold so that a sampler receives scalars instead of count arrays.
+ *   chi2    = cal_chi2 of p_devarshi24st.py:43-49: both arrays scaled by
+ *             fac = 1e6 / sum(m), chi2 = sum (fac d - fac m)^2 / (fac m);
+ *             entries with m <= 0 are left out (numpy gives inf/nan there)
+ *   loglike = Poisson log-likelihood sum (d ln m - m - lgamma(d + 1)); an
+ *             entry with m <= 0 adds -m when d == 0 and makes it -inf otherwise
+ * FP64 throughout, summed in a fixed order (bitwise reproducible). */
+typedef struct ppm_fit {
+  double chi2;
+  double loglike;
+  double model_total;   /* sum(m) */
+  int64_t n_zero_model; /* entries with m <= 0 */
+} ppm_fit;
+
+/* Registers observed counts [n_ch][n_bins] (the counts layout, n_ch of the
+ * response) and keeps them on the device; returns its id. */
+int ppm_engine_add_observed(ppm_engine* e, int32_t response, int32_t n_bins, const double* counts, int32_t* observed_id);
+/* Fit statistics of every profile of a batch after its last launch: enqueued
+ * on `stream` (NULL = the stream of the last launch), waits, writes n entries.
+ * Every profile must use the observed data's response and bin count. */
+int ppm_batch_fit(ppm_engine* e, ppm_batch* b, int32_t observed_id, ppm_fit* out, void* stream);
+/* Plain form: computes one profile and returns only its fit statistics. */
+int ppm_profile_fit(ppm_engine* e, const ppm_params* p, int32_t observed_id, ppm_fit* out, ppm_result_info* info);
 
 /* Sizes of the output arrays for a parameter set (doubles). */
 int ppm_output_sizes(ppm_engine* e, const ppm_params* p, int64_t* n_flux, int64_t* n_counts);

@@ -40,6 +40,9 @@ def _load(fast=False):
         L.oracle_profile.restype = ctypes.c_int
         L.oracle_profile.argtypes = [ctypes.c_void_p, ctypes.POINTER(_abi.Params), ctypes.c_int, _abi.DP, _abi.DP,
                                      ctypes.POINTER(_abi.ResultInfo)]
+        L.oracle_profile_rings.restype = ctypes.c_int
+        L.oracle_profile_rings.argtypes = [ctypes.c_void_p, ctypes.POINTER(_abi.Params), ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, _abi.DP, _abi.DP, ctypes.POINTER(_abi.ResultInfo)]
         L.oracle_profile_batch.restype = ctypes.c_int
         L.oracle_profile_batch.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(_abi.Params), ctypes.c_int,
                                            _abi.DP, _abi.DP, ctypes.POINTER(_abi.ResultInfo), ctypes.c_int]
@@ -79,6 +82,17 @@ class Oracle:
             raise RuntimeError(f"oracle_profile failed: {rc}")
         return flux, info
 
+    def profile_rings(self, p, e_obs, ring_begin, ring_end):
+        """The profile over HEALPix rings ring_begin <= i < ring_end only (point source: ring 0)."""
+        e = np.ascontiguousarray(e_obs, dtype=np.float64)
+        flux = np.zeros((p.n_bins, len(e)))
+        info = _abi.ResultInfo()
+        rc = self.L.oracle_profile_rings(self.ctx, ctypes.byref(p), ring_begin, ring_end, len(e), _abi.dptr(e),
+                                         _abi.dptr(flux), ctypes.byref(info))
+        if rc != 0:
+            raise RuntimeError(f"oracle_profile_rings failed: {rc}")
+        return flux, info
+
     def profile_batch(self, plist, e_obs, n_threads=1):
         e = np.ascontiguousarray(e_obs, dtype=np.float64)
         n = len(plist)
@@ -102,6 +116,33 @@ def fold(rsp, flux, exposure):
     counts = np.zeros((n_ch, n_bins))
     L.oracle_fold(n_ch, n_e, n_bins, _abi.dptr(rsp), _abi.dptr(flux), exposure, _abi.dptr(counts))
     return counts
+
+
+def cal_chi2(data, model):
+    """p_devarshi24st.py:43-49 (cal_chi2): both arrays scaled so the model sums to
+    1e6, chi2 = sum (data_ - model_)^2 / model_.  Entries with model <= 0 are left
+    out, as the engine's fit statistics document (numpy gives inf/nan there)."""
+    data = np.asarray(data, dtype=np.float64).ravel()
+    model = np.asarray(model, dtype=np.float64).ravel()
+    fac = 1e6 / np.sum(model)
+    keep = model > 0
+    model_ = model[keep] * fac
+    data_ = data[keep] * fac
+    return float(np.sum((data_ - model_) ** 2 / model_))
+
+
+def poisson_loglike(data, model):
+    """sum(d ln m - m - lgamma(d + 1)); entries with m <= 0 add -m when d == 0 and
+    give -inf otherwise."""
+    from math import lgamma
+
+    d = np.asarray(data, dtype=np.float64).ravel()
+    m = np.asarray(model, dtype=np.float64).ravel()
+    pos = m > 0
+    if np.any(~pos & (d != 0)):
+        return float("-inf")
+    lg = sum(lgamma(x + 1.0) for x in d)
+    return float(np.sum(d[pos] * np.log(m[pos]) - m[pos]) - np.sum(m[~pos]) - lg)
 
 
 def count_active(spot_struct, n_side):

@@ -396,9 +396,16 @@ typedef struct {
   double* phi;
 } oring;
 
-/* GenerateHealpixGrid (cpu/grid.hpp:194-250) or PointSource (cpu/grid.hpp:18-27). */
-static int build_grid(const ppm_spot* s, int N_side, oring** out, int* n_rings, int64_t* n_active) {
+/* GenerateHealpixGrid (cpu/grid.hpp:194-250) or PointSource (cpu/grid.hpp:18-27),
+ * restricted to rings ring_begin <= i < ring_end (a point source is ring 0). */
+static int build_grid(const ppm_spot* s, int N_side, int ring_begin, int ring_end, oring** out, int* n_rings,
+                      int64_t* n_active) {
   *n_active = 0;
+  if (s->kind == PPM_SPOT_POINT && !(ring_begin <= 0 && 0 < ring_end)) {
+    *out = NULL;
+    *n_rings = 0;
+    return 0;
+  }
   if (s->kind == PPM_SPOT_POINT) {
     oring* r = (oring*)calloc(1, sizeof(oring));
     double sin_half_ar = sin(0.5 * s->angrad1);
@@ -417,6 +424,7 @@ static int build_grid(const ppm_spot* s, int N_side, oring** out, int* n_rings, 
   double* buf = (double*)malloc(sizeof(double) * 4 * N_side);
   int nr = 0;
   for (int i = 1; i <= 4 * N_side - 1; ++i) {
+    if (i < ring_begin || i >= ring_end) continue;
     int m = i < 4 * N_side - i ? i : 4 * N_side - i;
     if (N_side < m) m = N_side;
     int jmax = 4 * m;
@@ -447,16 +455,17 @@ int64_t oracle_count_active(const ppm_spot* s, int N_side) {
   oring* rings;
   int nr;
   int64_t na;
-  build_grid(s, N_side, &rings, &nr, &na);
+  build_grid(s, N_side, 0, 4 * N_side, &rings, &nr, &na);
   for (int r = 0; r < nr; ++r) free(rings[r].phi);
   free(rings);
   return na;
 }
 
 /* ---- one profile ------------------------------------------------------------------ */
-/* flux[n_bins][n_e] accumulates the reference's total_flux(i_phase_bin, i_E). */
-int oracle_profile(const oracle_ctx* c, const ppm_params* p, int n_e, const double* E_obs, double* flux,
-                   ppm_result_info* info) {
+/* flux[n_bins][n_e] accumulates the reference's total_flux(i_phase_bin, i_E), over
+ * the HEALPix rings ring_begin <= i < ring_end only (a point source is ring 0). */
+int oracle_profile_rings(const oracle_ctx* c, const ppm_params* p, int ring_begin, int ring_end, int n_e,
+                         const double* E_obs, double* flux, ppm_result_info* info) {
   if (!c || !p || !E_obs || !flux) return PPM_E_INVALID;
   const int nsx = p->atmosphere == PPM_ATM_NSX;
   if (nsx && !c->has_nsx) return PPM_E_STATE;
@@ -498,7 +507,7 @@ int oracle_profile(const oracle_ctx* c, const ppm_params* p, int n_e, const doub
     oring* grid;
     int n_rings;
     int64_t n_act;
-    build_grid(s, p->n_side, &grid, &n_rings, &n_act);
+    build_grid(s, p->n_side, ring_begin, ring_end, &grid, &n_rings, &n_act);
     inf.n_active += n_act;
     inf.n_rings += n_rings;
 
@@ -697,6 +706,11 @@ int oracle_profile(const oracle_ctx* c, const ppm_params* p, int n_e, const doub
   free(MU);
   if (info) *info = inf;
   return PPM_OK;
+}
+
+int oracle_profile(const oracle_ctx* c, const ppm_params* p, int n_e, const double* E_obs, double* flux,
+                   ppm_result_info* info) {
+  return oracle_profile_rings(c, p, 0, 1 << 30, n_e, E_obs, flux, info);
 }
 
 /* cpu/devarshi24st_cpu.cpp:249-258: counts[ch][b] = sum_E flux[b][E] rsp[ch][E] * exposure * bin width */

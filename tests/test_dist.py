@@ -76,3 +76,64 @@ def test_shard_indices_cover_and_balance():
     costs = [10, 1, 1, 1, 1, 1, 1, 1, 1, 1]
     loads = [sum(costs[i] for i in pdist.shard_indices(10, r, 2, costs)) for r in range(2)]
     assert max(loads) == 10
+
+
+def _ring_worker(rank, world, port, out_q):
+    import torch.distributed as dist
+
+    import oracle
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    lens = synth.small_lensing()
+    E = synth.energy_grid(10, 0.5, 6.0)
+    p = synth.config1_params(0)
+    p.n_side = 16
+    p.n_bins = 8
+    windows = pdist.ring_partition(pdist.ring_costs(p), world)
+    ora = oracle.Oracle(lens)
+    part, _ = ora.profile_rings(p, E, *windows[rank])
+    total = pdist.reduce_sum_to_rank0([part])
+    if rank == 0:
+        full, _ = ora.profile(p, E)
+        err = float(np.max(np.abs(total[0] - full)) / np.max(np.abs(full)))
+        out_q.put((err, windows))
+    else:
+        out_q.put((0.0, windows))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_ring_split_reduces_to_full_profile():
+    """One profile split by HEALPix ring windows over two gloo ranks (the FP64
+    oracle stands in for each rank's engine): the sum-reduce to rank 0 equals
+    the whole profile."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_ring_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert max(e for e, _ in res) < 1e-12
+    w = res[0][1]
+    assert w[0][0] == 0 and w[0][1] == w[1][0] and w[1][1] == 4 * 16
+
+
+def test_ring_partition_balances_costs():
+    costs = np.array([0, 5, 5, 5, 5, 0, 0, 10, 10, 0], dtype=float)
+    for world in (1, 2, 3, 4):
+        win = pdist.ring_partition(costs, world)
+        assert win[0][0] == 0 and win[-1][1] == len(costs)
+        assert all(a[1] == b[0] for a, b in zip(win, win[1:]))
+        loads = [costs[b:e].sum() for b, e in win]
+        assert sum(loads) == costs.sum()
+        assert max(loads) <= costs.sum() / world + costs.max()
+    p = synth.config2_params(0, -1, n_side=32, n_bins=8)
+    import oracle
+
+    assert pdist.ring_costs(p).sum() == sum(oracle.count_active(p.spots[k], 32) for k in range(p.n_spots))

@@ -229,3 +229,41 @@ def test_table_edges_and_even_mu(monkeypatch, kernel):
                 assert info.n_points == oinfo.n_points and info.n_clamped > 0
                 assert max_rel(flux, ref) < TOL32, (axis, interp, len(E))
         e.close()
+
+
+def test_ring_windows_sum_to_full_profile(eng_v171019):
+    """ppm_profile_rings / ppm_batch_create_rings over a 3-way ring partition:
+    each window matches the oracle on the same rings and the windows sum to the
+    whole profile (FP64 fold, 1e-12); a point-source spot belongs to ring 0."""
+    from gpu_ppm_b200 import dist as pdist
+
+    g, r, E, rsp = eng_v171019.cfg2
+    p = synth.config2_params(g, r, n_side=48, n_bins=16, fold=_abi.FOLD_FP64)
+    full_f, full_c, _ = eng_v171019.profile(p)
+    wins = pdist.ring_partition(pdist.ring_costs(p), 3)
+    assert wins[0][0] == 0 and wins[-1][1] == 4 * 48
+    sf, sc = np.zeros_like(full_f), np.zeros_like(full_c)
+    for b, e in wins:
+        f, c, info = eng_v171019.profile_rings(p, b, e)
+        ref, oinfo = eng_v171019.ora.profile_rings(p, E, b, e)
+        assert info.n_points == oinfo.n_points
+        assert max_rel(f, ref) < TOL32, (b, e)
+        sf += f
+        sc += c
+    assert np.allclose(sf, full_f, rtol=1e-12, atol=1e-12 * np.abs(full_f).max())
+    assert np.allclose(sc, full_c, rtol=1e-12, atol=1e-12 * np.abs(full_c).max())
+    batch = eng_v171019.batch([p], rings=wins[1])
+    batch.launch()
+    bf, bc, _ = batch.collect(want_flux=True, want_counts=True)
+    f1, c1, _ = eng_v171019.profile_rings(p, *wins[1])
+    assert np.allclose(bf.reshape(f1.shape), f1, rtol=1e-12, atol=1e-300)
+    batch.close()
+    # point source: ring 0 only
+    q = synth.config2_params(g, r, n_side=48, n_bins=16, fold=_abi.FOLD_FP64)
+    q.n_spots = 1
+    q.spots[0].kind = _abi.SPOT_POINT
+    q.spots[0].angrad1 = 0.05
+    pf, _, _ = eng_v171019.profile(q)
+    f0, _, _ = eng_v171019.profile_rings(q, 0, 1)
+    f1, _, i1 = eng_v171019.profile_rings(q, 1, 4 * 48)
+    assert np.array_equal(f0, pf) and not f1.any() and i1.n_points == 0
