@@ -59,25 +59,72 @@ void DeviceBuffer::reserve(size_t bytes) {
   if (e != cudaSuccess) throw Error(PPM_E_OOM, std::string("cudaMalloc workspace: ") + cudaGetErrorString(e));
   cap = want;
 }
+void* BlockCache::get(size_t bytes, size_t* got) {
+  std::lock_guard<std::mutex> lk(m_);
+  auto it = free_.lower_bound(bytes);
+  if (it == free_.end() || it->first > 2 * bytes + (1u << 20)) return nullptr;
+  void* p = it->second;
+  *got = it->first;
+  held_ -= it->first;
+  free_.erase(it);
+  return p;
+}
+void BlockCache::put(void* p, size_t bytes) {
+  {
+    std::lock_guard<std::mutex> lk(m_);
+    if (held_ + bytes <= limit_) {
+      free_.emplace(bytes, p);
+      held_ += bytes;
+      return;
+    }
+  }
+  cudaFree(p);
+}
+void BlockCache::trim() {
+  std::lock_guard<std::mutex> lk(m_);
+  for (auto& kv : free_) cudaFree(kv.second);
+  free_.clear();
+  held_ = 0;
+}
+
 void* DeviceArena::alloc(size_t bytes) {
   void* p = nullptr;
-  cudaError_t e = stream ? cudaMallocAsync(&p, std::max<size_t>(bytes, 16), stream)
-                         : cudaMalloc(&p, std::max<size_t>(bytes, 16));
-  if (e != cudaSuccess) throw Error(PPM_E_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  size_t sz = std::max<size_t>(bytes, 16);
+  if (cache && !stream) {
+    // 64 KiB granules, so that blocks of batches of similar size fit one another
+    sz = (sz + 65535) / 65536 * 65536;
+    size_t got = 0;
+    p = cache->get(sz, &got);
+    if (p) sz = got;
+  }
+  if (!p) {
+    cudaError_t e = stream ? cudaMallocAsync(&p, sz, stream) : cudaMalloc(&p, sz);
+    if (e != cudaSuccess && cache && !stream) {  // give the cached blocks back and retry once
+      cudaGetLastError();
+      cache->trim();
+      e = cudaMalloc(&p, sz);
+    }
+    if (e != cudaSuccess) throw Error(PPM_E_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
   ptrs.push_back(p);
+  sizes.push_back(sz);
   bytes_held += bytes;
   return p;
 }
 DeviceArena::~DeviceArena() {
-  for (void* p : ptrs) {
+  for (size_t k = 0; k < ptrs.size(); ++k) {
     if (stream)
-      cudaFreeAsync(p, stream);
+      cudaFreeAsync(ptrs[k], stream);
+    else if (cache)
+      cache->put(ptrs[k], sizes[k]);
     else
-      cudaFree(p);
+      cudaFree(ptrs[k]);
   }
 }
 BatchImpl::~BatchImpl() {
   if (graph) cudaGraphExecDestroy(graph);
+  // cached blocks are handed to the next batch at once: the last launch must be done with them
+  if (mem.cache && !mem.stream && last_stream) cudaStreamSynchronize(last_stream);
 }
 
 void DeviceBuffer::release() {
@@ -104,6 +151,7 @@ Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   if (cfg.memory_budget <= 0) cfg.memory_budget = 64ll << 30;
   if (cfg.n_streams <= 0) cfg.n_streams = 4;
   if (cfg.max_batch <= 0) cfg.max_batch = 1 << 16;
+  block_cache.set_limit((size_t)cfg.memory_budget);
   int n_dev = 0;
   PPM_CUDA(cudaGetDeviceCount(&n_dev));
   if (cfg.device < 0 || cfg.device >= n_dev) throw Error(PPM_E_INVALID, "no such CUDA device");
@@ -126,6 +174,7 @@ Engine::~Engine() {
   cudaSetDevice(cfg.device);
   serve_shutdown();
   cudaStreamSynchronize(stream);
+  block_cache.trim();
   if (d_err) cudaFree(d_err);
   for (void* p : owned) cudaFree(p);
   for (auto& kv : ring_tabs) cudaFree(kv.second);
@@ -589,6 +638,7 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
                          int ring_end) {
   if (n < 1) throw Error(PPM_E_INVALID, "empty batch");
   if (ring_begin > ring_end) throw Error(PPM_E_INVALID, "ring window with begin > end");
+  if (!B.mem.stream) B.mem.cache = &block_cache;
   if (n > cfg.max_batch) throw Error(PPM_E_RANGE, "batch larger than max_batch");
   PPM_CUDA(cudaSetDevice(cfg.device));
   B.n = n;

@@ -70,10 +70,33 @@ struct Resp {
 };
 
 // Device allocations owned by one batch.
+// Device blocks released by synchronous batches, kept for the next batch so that
+// repeated ppm_profile / ppm_profile_batch calls do not pay cudaMalloc/cudaFree
+// (cudaFree synchronises the device).  A block is reused for a request of at
+// least half its size.  Thread-safe.
+class BlockCache {
+ public:
+  explicit BlockCache(size_t limit = 0) : limit_(limit) {}
+  ~BlockCache() { trim(); }
+  void set_limit(size_t limit) { limit_ = limit; }
+  // a cached block of at least `bytes` (its size in *got), or nullptr
+  void* get(size_t bytes, size_t* got);
+  // keeps the block (or frees it when the cache would exceed its limit)
+  void put(void* p, size_t bytes);
+  void trim();
+
+ private:
+  std::mutex m_;
+  std::multimap<size_t, void*> free_;
+  size_t held_ = 0, limit_ = 0;
+};
+
 struct DeviceArena {
   std::vector<void*> ptrs;
+  std::vector<size_t> sizes;
   size_t bytes_held = 0;
   cudaStream_t stream = nullptr;  // set: stream-ordered allocations (no implicit device synchronisation)
+  BlockCache* cache = nullptr;    // set (synchronous batches): blocks come from and return to the cache
   void* alloc(size_t bytes);
   DeviceArena() = default;
   DeviceArena(const DeviceArena&) = delete;
@@ -215,6 +238,7 @@ class Engine {
   std::vector<Grid> grids;
   std::vector<Resp> resps;
   std::vector<Observed> observed;
+  BlockCache block_cache;
   std::map<int, double*> ring_tabs, fine_tabs;
   std::map<int, std::vector<double>> host_rings;
   std::vector<void*> owned;

@@ -162,7 +162,8 @@ typedef struct ppm_engine ppm_engine;
 typedef struct ppm_engine_config {
   int32_t device;             /* CUDA device ordinal */
   int32_t max_batch;          /* largest batch ppm_profile_batch accepts (profiles) */
-  int64_t memory_budget;      /* bytes of device memory for in-flight request state (0 = 64 GiB) */
+  int64_t memory_budget;      /* bytes of device memory for in-flight request state (0 = 64 GiB); also
+                                 the most device memory the engine keeps cached between synchronous calls */
   int32_t autotune;           /* 1: time candidate launch shapes at first use */
   int32_t n_streams;          /* serving: concurrent batches in flight (0 = 4) */
 } ppm_engine_config;
