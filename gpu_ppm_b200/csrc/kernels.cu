@@ -583,27 +583,6 @@ __device__ __forceinline__ void cell_polys(const float* Sx, int ldS, int nE, int
   }
 }
 
-// Packed FP32 pairs (fma/add .f32x2): two records' values in one register pair.
-typedef unsigned long long f32x2;
-__device__ __forceinline__ f32x2 pk(float lo, float hi) {
-  f32x2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ void upk(f32x2 v, float& lo, float& hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
-  f32x2 d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
-  f32x2 d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-
 template <int MAXE, int NTMAX, int MINB>
 __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const KernelArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
@@ -716,16 +695,15 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
       e0 = G.cell_first[r];
       cnt = min(G.cell_first[r + 1] - e0, MAXE);
     }
-    // per energy slot: its fraction in both halves, and partial sums of the
-    // even (low half) and odd (high half) records of a record pair
-    f32x2 fEb[MAXE], acc[MAXE];
+    // per energy slot: its fraction, and partial sums of the first and the
+    // second record of the record pairs
+    float fEv[MAXE], accA[MAXE], accB[MAXE];
 #pragma unroll
     for (int k = 0; k < MAXE; ++k) {
-      const float f = k < cnt ? G.fEs[e0 + k] : 0.f;
-      fEb[k] = pk(f, f);
-      acc[k] = pk(0.f, 0.f);
+      fEv[k] = k < cnt ? G.fEs[e0 + k] : 0.f;
+      accA[k] = 0.f;
+      accB[k] = 0.f;
     }
-    const f32x2 minus1 = pk(-1.f, -1.f);
     const int mode = p.interp;
     const bool cubicE = mode != 4;
     const bool sg = mode == 1;
@@ -739,14 +717,13 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
     auto flush = [&]() {
 #pragma unroll
       for (int k = 0; k < MAXE; ++k) {
-        float lo, hi;
-        upk(acc[k], lo, hi);
-        const float v = lo + hi;
+        const float v = accA[k] + accB[k];
         if (k < cnt && v != 0.f) {
           const int e = G.perm[e0 + k];
           atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)v * out_scale * G.invE[e]);
         }
-        acc[k] = pk(0.f, 0.f);
+        accA[k] = 0.f;
+        accB[k] = 0.f;
       }
     };
 
@@ -809,8 +786,9 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
       }
 
       // each warp set takes a contiguous run of the records (one flush per bin
-      // change in its run) in pairs of same-bin records, the two halves of
-      // packed FP32 pairs; a record without a partner pairs with itself at weight 0
+      // change in its run) in pairs of same-bin records interleaved for
+      // instruction-level parallelism; a record without a partner pairs with
+      // itself at weight 0
       const int b_end = (int)((long long)nv * (set + 1) / n_sets);
       for (int b = (int)((long long)nv * set / n_sets); b < b_end;) {
         const float4 rA = rec[2 * b], wA = rec[2 * b + 1];
@@ -837,28 +815,26 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
           rB.x = 0.f;
         }
         b += two ? 2 : 1;
-        const f32x2 cw = pk(rA.x, rB.x), fP = pk(rA.y, rB.y);
-        const f32x2 p0x = pk(A0.x, B0.x), p0y = pk(A0.y, B0.y), p0z = pk(A0.z, B0.z), p0w = pk(A0.w, B0.w);
-        const f32x2 p1x = pk(A1.x, B1.x), p1y = pk(A1.y, B1.y), p1z = pk(A1.z, B1.z), p1w = pk(A1.w, B1.w);
 #pragma unroll
         for (int k = 0; k < MAXE; ++k) {
-          // split coordinate t = fE + fP: cell G0 + r below 1, cell G0 + r + 1 at t - 1 above
-          const f32x2 t0 = add2(fEb[k], fP), t1 = add2(t0, minus1);
-          const f32x2 v0 = fma2(fma2(fma2(p0w, t0, p0z), t0, p0y), t0, p0x);
-          const f32x2 v1 = fma2(fma2(fma2(p1w, t1, p1z), t1, p1y), t1, p1x);
-          float ta, tb, a0, b0, a1, b1;
-          upk(t0, ta, tb);
-          upk(v0, a0, b0);
-          upk(v1, a1, b1);
+          // split coordinate t = fE + fP: cell G0 + r below 1, cell G0 + r + 1 at t - 1
+          // above; both cubics are evaluated and the result selected
+          const float ta = fEv[k] + rA.y, tb = fEv[k] + rB.y, ta1 = ta - 1.f, tb1 = tb - 1.f;
+          const float a0 = fmaf(fmaf(fmaf(A0.w, ta, A0.z), ta, A0.y), ta, A0.x);
+          const float a1 = fmaf(fmaf(fmaf(A1.w, ta1, A1.z), ta1, A1.y), ta1, A1.x);
+          const float b0 = fmaf(fmaf(fmaf(B0.w, tb, B0.z), tb, B0.y), tb, B0.x);
+          const float b1 = fmaf(fmaf(fmaf(B1.w, tb1, B1.z), tb1, B1.y), tb1, B1.x);
           float va = ta >= 1.f ? a1 : a0, vb = tb >= 1.f ? b1 : b0;
           if (sg) {
             va = fmaxf(va, 0.f);
             vb = fmaxf(vb, 0.f);
           }
-          acc[k] = fma2(cw, pk(va, vb), acc[k]);
+          accA[k] = fmaf(rA.x, va, accA[k]);
+          accB[k] = fmaf(rB.x, vb, accB[k]);
         }
       }
-      __syncthreads();
+      // no barrier here: the next round writes records only after the barriers
+      // of its compaction, which every warp reaches after this loop
     }
     if (cur_bin >= 0) flush();
   }

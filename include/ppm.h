@@ -276,7 +276,8 @@ int ppm_engine_autotune(ppm_engine* e, int32_t n, const ppm_params* sample, char
  *             entries with m <= 0 are left out (numpy gives inf/nan there)
  *   loglike = Poisson log-likelihood sum (d ln m - m - lgamma(d + 1)); an
  *             entry with m <= 0 adds -m when d == 0 and makes it -inf otherwise
- * FP64 throughout, summed in a fixed order (bitwise reproducible). */
+ * FP64 throughout, summed in a fixed order (equal counts give bitwise equal
+ * statistics). */
 typedef struct ppm_fit {
   double chi2;
   double loglike;
