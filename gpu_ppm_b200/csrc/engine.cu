@@ -158,13 +158,14 @@ Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   PPM_CUDA(cudaSetDevice(cfg.device));
   PPM_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, cfg.device));
   PPM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-  // launch-shape overrides for experiments: PPM_PB, PPM_CHUNK, PPM_NE_T, PPM_MINB, PPM_KERNEL, PPM_SETS
+  // launch-shape overrides for experiments: PPM_PB, PPM_CHUNK, PPM_NE_T, PPM_MINB, PPM_KERNEL, PPM_SETS, PPM_CPL
   if (const char* v = std::getenv("PPM_PB")) tune.pb = std::max(1, std::atoi(v));
   if (const char* v = std::getenv("PPM_CHUNK")) tune.chunk = std::max(32, std::atoi(v));
   if (const char* v = std::getenv("PPM_NE_T")) tune.ne_t = std::atoi(v);
-  if (const char* v = std::getenv("PPM_MINB")) tune.minb = std::max(1, std::min(3, std::atoi(v)));
+  if (const char* v = std::getenv("PPM_MINB")) tune.minb = std::max(1, std::min(2, std::atoi(v)));
   if (const char* v = std::getenv("PPM_KERNEL")) tune.kernel = std::atoi(v) ? 1 : 0;
   if (const char* v = std::getenv("PPM_SETS")) tune.sets = std::max(0, std::atoi(v));
+  if (const char* v = std::getenv("PPM_CPL")) tune.cpl = std::max(0, std::min(3, std::atoi(v)));
   for (int k = 0; k < 4; ++k) PPM_CUDA(cudaEventCreate(&ev[k]));
   PPM_CUDA(cudaMalloc(&d_err, sizeof(int)));
   PPM_CUDA(cudaMemset(d_err, 0, sizeof(int)));
@@ -906,13 +907,29 @@ void Engine::profile_batch(int n, const ppm_params* ps, double* flux, double* co
 
 IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max, int maxe_max,
                                     int bins_max) {
-  // home-cell NSX kernel: one warp per 32 cells of a point, warp sets up to 512 threads
+  // home-cell NSX kernel: cpl cells per lane, 32 cpl per warp, warp sets up to 512 threads
   const int span_max = cells_max - 1;
-  const int cell_warps = (span_max + kCellsPerWarp - 1) / kCellsPerWarp;
-  if (nsx_kernel && tune.kernel == 0 && maxe_max >= 1 && maxe_max <= 16 && cell_warps <= 16 && nsx.nmu < 4096 &&
+  const int maxe_t = maxe_max <= 4 ? 4 : (maxe_max <= 8 ? 8 : 16);
+  if (nsx_kernel && tune.kernel == 0 && maxe_max >= 1 && maxe_max <= 16 && span_max <= 16 * 32 && nsx.nmu < 4096 &&
       bins_max < (1 << 20)) {
-    // default: about 384 threads (two CTAs of 80 registers per SM measured fastest)
-    int sets = std::min(16 / cell_warps, tune.sets > 0 ? tune.sets : std::max(1, 12 / cell_warps));
+    // cells per lane: fewest estimated lane instructions per point (window rows,
+    // polynomials, record handling, energy slots), over what the slots' registers allow
+    const int cmax = maxe_t == 4 ? 3 : (maxe_t == 8 ? 2 : 1);
+    int cpl = 1;
+    long best = -1;
+    for (int c = 1; c <= cmax; ++c) {
+      const long w = (span_max + 32 * c - 1) / (32 * c);
+      if (w > 16) continue;
+      const long cost = w * (20 * (c + 1) + 30 + 11L * maxe_t * c);
+      if (best < 0 || cost < best) {
+        best = cost;
+        cpl = c;
+      }
+    }
+    if (tune.cpl > 0) cpl = std::min(tune.cpl, cmax);
+    const int cell_warps = (span_max + 32 * cpl - 1) / (32 * cpl);
+    // default: about 256 threads (three CTAs of 80 registers per SM measured fastest)
+    int sets = std::min(16 / cell_warps, tune.sets > 0 ? tune.sets : std::max(1, 8 / cell_warps));
     IntegrandShape s;
     for (;;) {
       const int nt = 32 * cell_warps * sets;
@@ -922,8 +939,9 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
     }
     s.bb_fp64 = 0;
     s.cell_warps = cell_warps;
-    s.maxe_t = maxe_max <= 4 ? 4 : (maxe_max <= 8 ? 8 : 16);
-    s.minb = s.maxe_t <= 8 ? tune.minb : 1;
+    s.cpl = cpl;
+    s.maxe_t = maxe_t;
+    s.minb = maxe_t <= 8 ? tune.minb : 1;
     return s;
   }
   int ne_t = 1;
@@ -970,8 +988,8 @@ std::string Engine::autotune(int n, const ppm_params* sample) {
   std::string rep;
   auto line = [&](const Tuning& t, float ms, const char* note) {
     char buf[160];
-    std::snprintf(buf, sizeof(buf), "pb=%d chunk=%d minb=%d ne_t=%d sets=%d kernel=%d : %.3f ms%s\n", t.pb, t.chunk,
-                  t.minb, t.ne_t, t.sets, t.kernel, ms, note);
+    std::snprintf(buf, sizeof(buf), "pb=%d chunk=%d minb=%d ne_t=%d sets=%d cpl=%d kernel=%d : %.3f ms%s\n", t.pb,
+                  t.chunk, t.minb, t.ne_t, t.sets, t.cpl, t.kernel, ms, note);
     rep += buf;
   };
   Tuning best = start;
@@ -980,9 +998,10 @@ std::string Engine::autotune(int n, const ppm_params* sample) {
   const std::vector<std::pair<int Tuning::*, std::vector<int>>> dims = {
       {&Tuning::pb, {10, 20, 30, 40}},
       {&Tuning::chunk, {256, 512, 1024, 2048}},
-      {&Tuning::minb, {1, 2, 3}},
+      {&Tuning::minb, {1, 2}},
       {&Tuning::ne_t, {0, 2}},
       {&Tuning::sets, {0, 1, 2, 3, 4}},
+      {&Tuning::cpl, {0, 1, 2, 3}},
       {&Tuning::kernel, {0, 1}},
   };
   for (const auto& d : dims) {

@@ -150,9 +150,10 @@ struct Tuning {
   int pb = 20;       // phase points per polynomial sub-batch (rounded to whole warps)
   int chunk = 1024;  // candidate elements per tile
   int ne_t = 0;      // energies per thread (0 = automatic)
-  int minb = 2;      // CTAs per SM targeted by the register budget (3: home-cell kernel with <= 256 threads only)
+  int minb = 2;      // CTAs per SM targeted by the register budget
   int kernel = 0;    // NSX integrand: 0 = home-cell kernel where the grid allows, 1 = pooled-polynomial kernel
-  int sets = 0;      // home-cell kernel: warp sets per CTA (0 = about 384 threads)
+  int sets = 0;      // home-cell kernel: warp sets per CTA (0 = about 256 threads)
+  int cpl = 0;       // home-cell kernel: cells per lane (0 = by estimated cost)
 };
 
 // Observed counts [n_ch][n_bins] for fit statistics.

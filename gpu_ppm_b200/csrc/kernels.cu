@@ -545,45 +545,37 @@ __device__ __forceinline__ float4 cubic_cell(float h0, float h1, float h2, float
   return make_float4(h2, d1 + 1.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 + 0.5f * d3, c3);
 }
 
-// Polynomials of cells G0 + r and G0 + r + 1 for one point record; called by
-// the whole warp (shuffles).  rec = {c, fP, bin | imu << 20, G0}, w = mu weights.
+// Slice rows seen by one lane for one point record.  The lane owns C
+// consecutive cells starting at cell g (= G0 + first cell of the lane) and
+// needs the cubics of cells g .. g + C, i.e. rows g - 1 .. g + C + 2 of the
+// mu-contracted slice: window h[j] = row g - 1 + j, j = 0 .. C + 3.  The lane
+// contracts rows j < C itself; row j >= C is own row j mod C of lane
+// lane + j / C, or, past the end of the warp, one of the four rows after the
+// warp's last own row, which lanes 28..31 contract.
 // Sx points at slice row 0 of a slice with rows -2 .. nE + 1: rows -1 and nE
 // hold the cubic extrapolations of the first and last four rows, so that the
 // centred stencil of cell 0 (rows -1..2) and of cell nE - 2 (rows nE - 3..nE)
 // is the same cubic as the end-clamped stencil (rows 0..3, rows nE - 4..nE - 1);
 // rows -2 and nE + 1 repeat rows 0 and nE - 1, and window rows are clamped to
 // -2 .. nE + 1, so cells past either end see the end value H[0] / H[nE - 1].
-// Every lane contracts two rows, j = 0 (h0) and j = 4 (h4) of its window
-// G0 + r - 1 + j; row j of lane l is h0 of lane l + j, or h4 of lane
-// l + j - 4 past the end of the warp.
-__device__ __forceinline__ void cell_polys(const float* Sx, int ldS, int nE, int r, int lane, bool cubicE, float4 rec,
-                                           float4 w, float4& Q0, float4& Q1) {
-  const int imu = (int)(__float_as_uint(rec.z) >> 20);
-  const int g = __float_as_int(rec.w) + r;
-  const float h0 = slice_dot(Sx, ldS, min(max(g - 1, -2), nE + 1), imu, w);
-  const float h4 = slice_dot(Sx, ldS, min(max(g + 3, -2), nE + 1), imu, w);
-  const float a1 = __shfl_down_sync(0xffffffffu, h0, 1), b1 = __shfl_sync(0xffffffffu, h4, (lane - 3) & 31);
-  const float a2 = __shfl_down_sync(0xffffffffu, h0, 2), b2 = __shfl_sync(0xffffffffu, h4, (lane - 2) & 31);
-  const float a3 = __shfl_down_sync(0xffffffffu, h0, 3), b3 = __shfl_sync(0xffffffffu, h4, (lane - 1) & 31);
-  const float h1 = lane < 31 ? a1 : b1, h2 = lane < 30 ? a2 : b2, h3 = lane < 29 ? a3 : b3;
-  if (cubicE) {
-    Q0 = cubic_cell(h0, h1, h2, h3, 1);
-    Q1 = cubic_cell(h1, h2, h3, h4, 1);
-  } else {
-    Q0 = make_float4(h1, h2 - h1, 0.f, 0.f);
-    Q1 = make_float4(h2, h3 - h2, 0.f, 0.f);
-  }
-  // cells past an end hold the end value: H[0] is h0 there; H[nE - 1] is h1,
-  // except where window row 1 is the extrapolated row nE
-  if (__any_sync(0xffffffffu, (unsigned)g > (unsigned)(nE - 3))) {
-    if (g < 0) Q0 = make_float4(h0, 0.f, 0.f, 0.f);
-    if (g > nE - 2) Q0 = make_float4(g == nE ? h0 : h1, 0.f, 0.f, 0.f);
-    if (g < -1) Q1 = make_float4(h0, 0.f, 0.f, 0.f);
-    if (g > nE - 3) Q1 = make_float4(g == nE - 1 ? h1 : h2, 0.f, 0.f, 0.f);
+template <int C>
+__device__ __forceinline__ void lane_window(const float* Sx, int ldS, int nE, int lane, int g, int gw, int imu,
+                                            float4 w, float (&h)[C + 4]) {
+#pragma unroll
+  for (int j = 0; j < C; ++j) h[j] = slice_dot(Sx, ldS, min(max(g - 1 + j, -2), nE + 1), imu, w);
+  // rows gw + 32 C - 1 + m, m = 0..3 (gw = G0 + first cell of the warp)
+  float xr = 0.f;
+  if (lane >= 28) xr = slice_dot(Sx, ldS, min(max(gw + 32 * C - 1 + (lane - 28), -2), nE + 1), imu, w);
+#pragma unroll
+  for (int j = C; j < C + 4; ++j) {
+    const int q = j / C, jj = j - q * C;
+    const float own = __shfl_down_sync(0xffffffffu, h[jj], q);
+    const float extra = __shfl_sync(0xffffffffu, xr, (C * lane + j - 32 * C + 28) & 31);
+    h[j] = lane + q < 32 ? own : extra;
   }
 }
 
-template <int MAXE, int NTMAX, int MINB>
+template <int MAXE, int C, int NTMAX, int MINB>
 __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const KernelArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
   const IntegrandShape& S = a.shape;
@@ -599,7 +591,8 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
   const int nE = X.nE, nmu = X.nmu, ldS = S.ldS;
   const int lane = tid & 31, warp = tid >> 5;
   const int set = warp / S.cell_warps, n_sets = (nt >> 5) / S.cell_warps;
-  const int r = (warp - set * S.cell_warps) * kCellsPerWarp + lane;  // home cell
+  const int wc = (warp - set * S.cell_warps) * 32 * C;  // first cell of the warp
+  const int r0 = wc + C * lane;                         // first of the lane's C home cells
   float4* rec = (float4*)s.batch;  // [nt][2]: {c, fP, bin | imu << 20, G0}, {mu weights}
 
   for (;;) {
@@ -690,19 +683,19 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
     // ---- deposit
     const DevGrid& G = p.grid;
     const int n_e = G.n_e;
-    int e0 = 0, cnt = 0;
-    if (r < G.span) {
-      e0 = G.cell_first[r];
-      cnt = min(G.cell_first[r + 1] - e0, MAXE);
-    }
-    // per energy slot: its fraction, and partial sums of the first and the
-    // second record of the record pairs
-    float fEv[MAXE], accA[MAXE], accB[MAXE];
+    // per home cell i of the lane: its energies (MAXE slots: fraction, partial sum)
+    int e0[C], cnt[C];
+    float fEv[C][MAXE], acc[C][MAXE];
 #pragma unroll
-    for (int k = 0; k < MAXE; ++k) {
-      fEv[k] = k < cnt ? G.fEs[e0 + k] : 0.f;
-      accA[k] = 0.f;
-      accB[k] = 0.f;
+    for (int i = 0; i < C; ++i) {
+      const int rc = r0 + i;
+      e0[i] = rc < G.span ? G.cell_first[rc] : 0;
+      cnt[i] = rc < G.span ? min(G.cell_first[rc + 1] - e0[i], MAXE) : 0;
+#pragma unroll
+      for (int k = 0; k < MAXE; ++k) {
+        fEv[i][k] = k < cnt[i] ? G.fEs[e0[i] + k] : 0.f;
+        acc[i][k] = 0.f;
+      }
     }
     const int mode = p.interp;
     const bool cubicE = mode != 4;
@@ -716,15 +709,15 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
 
     auto flush = [&]() {
 #pragma unroll
-      for (int k = 0; k < MAXE; ++k) {
-        const float v = accA[k] + accB[k];
-        if (k < cnt && v != 0.f) {
-          const int e = G.perm[e0 + k];
-          atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)v * out_scale * G.invE[e]);
+      for (int i = 0; i < C; ++i)
+#pragma unroll
+        for (int k = 0; k < MAXE; ++k) {
+          if (k < cnt[i] && acc[i][k] != 0.f) {
+            const int e = G.perm[e0[i] + k];
+            atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)acc[i][k] * out_scale * G.invE[e]);
+          }
+          acc[i][k] = 0.f;
         }
-        accA[k] = 0.f;
-        accB[k] = 0.f;
-      }
     };
 
     const double* den = s.mu + nmu;  // [nmu - 3][4] reciprocal Lagrange denominators
@@ -786,52 +779,48 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
       }
 
       // each warp set takes a contiguous run of the records (one flush per bin
-      // change in its run) in pairs of same-bin records interleaved for
-      // instruction-level parallelism; a record without a partner pairs with
-      // itself at weight 0
+      // change in its run)
       const int b_end = (int)((long long)nv * (set + 1) / n_sets);
-      for (int b = (int)((long long)nv * set / n_sets); b < b_end;) {
+      for (int b = (int)((long long)nv * set / n_sets); b < b_end; ++b) {
         const float4 rA = rec[2 * b], wA = rec[2 * b + 1];
-        const int binA = (int)(__float_as_uint(rA.z) & 0xFFFFFu);
-        if (binA != cur_bin) {
+        const unsigned packed = __float_as_uint(rA.z);
+        const int bin = (int)(packed & 0xFFFFFu);
+        if (bin != cur_bin) {
           if (cur_bin >= 0) flush();
-          cur_bin = binA;
+          cur_bin = bin;
         }
-        bool two = false;
-        float4 rB = rA, wB = wA;
-        if (b + 1 < b_end) {
-          rB = rec[2 * b + 2];
-          wB = rec[2 * b + 3];
-          two = (int)(__float_as_uint(rB.z) & 0xFFFFFu) == binA;
-        }
-        float4 A0, A1, B0, B1;
-        cell_polys(Sx, ldS, nE, r, lane, cubicE, rA, wA, A0, A1);
-        if (two) {
-          cell_polys(Sx, ldS, nE, r, lane, cubicE, rB, wB, B0, B1);
-        } else {
-          B0 = A0;
-          B1 = A1;
-          rB = rA;
-          rB.x = 0.f;
-        }
-        b += two ? 2 : 1;
+        const int g = __float_as_int(rA.w) + r0;  // first home cell of the lane for this point
+        float h[C + 4];
+        lane_window<C>(Sx, ldS, nE, lane, g, __float_as_int(rA.w) + wc, (int)(packed >> 20), wA, h);
+        float4 Q[C + 1];
 #pragma unroll
-        for (int k = 0; k < MAXE; ++k) {
-          // split coordinate t = fE + fP: cell G0 + r below 1, cell G0 + r + 1 at t - 1
-          // above; both cubics are evaluated and the result selected
-          const float ta = fEv[k] + rA.y, tb = fEv[k] + rB.y, ta1 = ta - 1.f, tb1 = tb - 1.f;
-          const float a0 = fmaf(fmaf(fmaf(A0.w, ta, A0.z), ta, A0.y), ta, A0.x);
-          const float a1 = fmaf(fmaf(fmaf(A1.w, ta1, A1.z), ta1, A1.y), ta1, A1.x);
-          const float b0 = fmaf(fmaf(fmaf(B0.w, tb, B0.z), tb, B0.y), tb, B0.x);
-          const float b1 = fmaf(fmaf(fmaf(B1.w, tb1, B1.z), tb1, B1.y), tb1, B1.x);
-          float va = ta >= 1.f ? a1 : a0, vb = tb >= 1.f ? b1 : b0;
-          if (sg) {
-            va = fmaxf(va, 0.f);
-            vb = fmaxf(vb, 0.f);
+        for (int i = 0; i <= C; ++i)
+          Q[i] = cubicE ? cubic_cell(h[i], h[i + 1], h[i + 2], h[i + 3], 1)
+                        : make_float4(h[i + 1], h[i + 2] - h[i + 1], 0.f, 0.f);
+        // cells past an end hold the end value: H[0] is h[i] there; H[nE - 1]
+        // is h[i + 1], except where that window row is the extrapolated row nE
+        if (__any_sync(0xffffffffu, g < 0 || g + C > nE - 2)) {
+#pragma unroll
+          for (int i = 0; i <= C; ++i) {
+            const int gi = g + i;
+            if (gi < 0) Q[i] = make_float4(h[i], 0.f, 0.f, 0.f);
+            if (gi > nE - 2) Q[i] = make_float4(gi == nE ? h[i] : h[i + 1], 0.f, 0.f, 0.f);
           }
-          accA[k] = fmaf(rA.x, va, accA[k]);
-          accB[k] = fmaf(rB.x, vb, accB[k]);
         }
+        const float cw = rA.x, fP = rA.y;
+#pragma unroll
+        for (int i = 0; i < C; ++i)
+#pragma unroll
+          for (int k = 0; k < MAXE; ++k) {
+            // split coordinate t = fE + fP: cell i below 1, cell i + 1 at t - 1
+            // above; both cubics are evaluated and the result selected
+            const float t = fEv[i][k] + fP, t1 = t - 1.f;
+            const float v0 = fmaf(fmaf(fmaf(Q[i].w, t, Q[i].z), t, Q[i].y), t, Q[i].x);
+            const float v1 = fmaf(fmaf(fmaf(Q[i + 1].w, t1, Q[i + 1].z), t1, Q[i + 1].y), t1, Q[i + 1].x);
+            float v = t >= 1.f ? v1 : v0;
+            if (sg) v = fmaxf(v, 0.f);
+            acc[i][k] = fmaf(cw, v, acc[i][k]);
+          }
       }
       // no barrier here: the next round writes records only after the barriers
       // of its compaction, which every warp reaches after this loop
@@ -1158,19 +1147,18 @@ IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int 
 namespace {
 void* kernel_for(const IntegrandShape& s, int precision) {
   if (s.nsx && s.cellk) {
-    // register budget: CTAs per SM (minb) at the launch's thread count
-    const int v = s.minb >= 3 && s.nt <= 256 ? 3 : (s.minb >= 2 ? (s.nt <= 384 ? 2 : 1) : 0);
+    // register budget: two CTAs per SM (80 registers) up to 384 threads, else one
+    const bool two = s.minb >= 2 && s.nt <= 384;
     if (s.maxe_t == 4) {
-      void* f[] = {(void*)integrand_nsx_cell_kernel<4, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 512, 2>,
-                   (void*)integrand_nsx_cell_kernel<4, 384, 2>, (void*)integrand_nsx_cell_kernel<4, 256, 3>};
-      return f[v];
+      if (s.cpl >= 3) return two ? (void*)integrand_nsx_cell_kernel<4, 3, 384, 2> : (void*)integrand_nsx_cell_kernel<4, 3, 512, 1>;
+      if (s.cpl == 2) return two ? (void*)integrand_nsx_cell_kernel<4, 2, 384, 2> : (void*)integrand_nsx_cell_kernel<4, 2, 512, 1>;
+      return two ? (void*)integrand_nsx_cell_kernel<4, 1, 384, 2> : (void*)integrand_nsx_cell_kernel<4, 1, 512, 1>;
     }
     if (s.maxe_t == 8) {
-      void* f[] = {(void*)integrand_nsx_cell_kernel<8, 512, 1>, (void*)integrand_nsx_cell_kernel<8, 512, 2>,
-                   (void*)integrand_nsx_cell_kernel<8, 384, 2>, (void*)integrand_nsx_cell_kernel<8, 256, 3>};
-      return f[v];
+      if (s.cpl >= 2) return two ? (void*)integrand_nsx_cell_kernel<8, 2, 384, 2> : (void*)integrand_nsx_cell_kernel<8, 2, 512, 1>;
+      return two ? (void*)integrand_nsx_cell_kernel<8, 1, 384, 2> : (void*)integrand_nsx_cell_kernel<8, 1, 512, 1>;
     }
-    return (void*)integrand_nsx_cell_kernel<16, 512, 1>;
+    return (void*)integrand_nsx_cell_kernel<16, 1, 512, 1>;
   }
   if (s.nsx) {
     const bool two = s.minb >= 2;
@@ -1199,11 +1187,12 @@ cudaError_t configure_integrand_smem(const IntegrandShape& s) {
   // all variants get the largest dynamic shared memory allowance once
   static bool done = false;
   if (done) return cudaSuccess;
-  void* fns[] = {(void*)integrand_nsx_cell_kernel<4, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 512, 2>,
-                 (void*)integrand_nsx_cell_kernel<4, 384, 2>, (void*)integrand_nsx_cell_kernel<4, 256, 3>,
-                 (void*)integrand_nsx_cell_kernel<8, 512, 1>, (void*)integrand_nsx_cell_kernel<8, 512, 2>,
-                 (void*)integrand_nsx_cell_kernel<8, 384, 2>, (void*)integrand_nsx_cell_kernel<8, 256, 3>,
-                 (void*)integrand_nsx_cell_kernel<16, 512, 1>,
+  void* fns[] = {(void*)integrand_nsx_cell_kernel<4, 1, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 1, 384, 2>,
+                 (void*)integrand_nsx_cell_kernel<4, 2, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 2, 384, 2>,
+                 (void*)integrand_nsx_cell_kernel<4, 3, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 3, 384, 2>,
+                 (void*)integrand_nsx_cell_kernel<8, 1, 512, 1>, (void*)integrand_nsx_cell_kernel<8, 1, 384, 2>,
+                 (void*)integrand_nsx_cell_kernel<8, 2, 512, 1>, (void*)integrand_nsx_cell_kernel<8, 2, 384, 2>,
+                 (void*)integrand_nsx_cell_kernel<16, 1, 512, 1>,
                  (void*)integrand_nsx_kernel<1, 1>, (void*)integrand_nsx_kernel<1, 2>,
                  (void*)integrand_nsx_kernel<2, 1>, (void*)integrand_nsx_kernel<2, 2>, (void*)integrand_nsx_kernel<4, 1>,
                  (void*)integrand_bb_kernel<double, 1>, (void*)integrand_bb_kernel<double, 2>,

@@ -24,7 +24,8 @@ struct IntegrandShape {
   // home-cell NSX kernel: one lane per energy cell, record groups of cell_warps warps
   int cellk;      // 1 = home-cell kernel, 0 = pooled-polynomial kernel
   int maxe_t;     // energies per lane the home-cell kernel is compiled for (4, 8, 16)
-  int cell_warps; // warps covering the cells of one point (32 cells per warp)
+  int cell_warps; // warps covering the cells of one point (32 x cpl cells per warp)
+  int cpl;        // home cells per lane (1..3)
   int ldS;        // floats between the slice rows in shared memory (odd: conflict-free column reads)
   // offsets in bytes
   int off_j, off_P, off_F, off_Z, off_MU, off_mu, off_S, off_union, off_rows, off_batch, off_Q, total;
@@ -32,8 +33,6 @@ struct IntegrandShape {
 
 IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int n_fine, int n_cp, int n_ca, int nE,
                           int nmu, int cells, bool cellk = false);
-// cells the lanes of one warp of the home-cell kernel own
-constexpr int kCellsPerWarp = 32;
 
 struct KernelArgs {
   const DevProfile* profiles;
