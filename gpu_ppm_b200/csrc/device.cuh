@@ -148,15 +148,24 @@ __device__ __forceinline__ void cubic_lagrange(double w[4], double x, double x0,
 
 __device__ __forceinline__ double uhunt_at(double lo, double hi, int n, int i) { return lo + (hi - lo) * i / (n - 1); }
 
-// HEALPix azimuth of element j in ring i (cpu/grid.hpp:219-244, gpu/healpix.cuh:74-91).
-__device__ __forceinline__ double healpix_phi(int N, int i, int j) {
+// HEALPix azimuth of element j in ring i, phi = dphi * (j - jofs)
+// (cpu/grid.hpp:219-244, gpu/healpix.cuh:74-91): the per-ring factors, so that
+// a loop over the elements of one ring evaluates the same expression.
+struct RingPhi {
+  double dphi, jofs;
+};
+__device__ __forceinline__ RingPhi healpix_ring_phi(int N, int i) {
   if (i > 2 * N) i = 4 * N - i;
   if (i < N) {
     double s = 1.;
-    return 3.14159265358979323846 / (2. * i) * (j - s / 2.);
+    return RingPhi{3.14159265358979323846 / (2. * i), s / 2.};
   }
   double s = (i - N + 1) % 2;
-  return 3.14159265358979323846 / (2. * N) * (j - s / 2.);
+  return RingPhi{3.14159265358979323846 / (2. * N), s / 2.};
+}
+__device__ __forceinline__ double healpix_phi(int N, int i, int j) {
+  const RingPhi r = healpix_ring_phi(N, i);
+  return r.dphi * (j - r.jofs);
 }
 
 __device__ __forceinline__ int healpix_jmax(int N, int i) {

@@ -180,8 +180,8 @@ __device__ int tile_prologue(const KernelArgs& a, const DevProfile& p, const Dev
 
 // Phase point q of the tile: GL node (or sample phase), patch phase, hunt and
 // lerps in FP64 (cpu/devarshi24st_cpu.cpp:214-229).  Returns flux/I (0 = skip).
-__device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtrs& s, int ring, bool point, int n_act,
-                                              int q, int& bin, double& wgl, double& z, double& mu) {
+__device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtrs& s, const RingPhi& rp, bool point,
+                                              int n_act, int q, int& bin, double& wgl, double& z, double& mu) {
   const int n_gl = p.n_gl;
   const int i_pp = q / n_act, jj = q - i_pp * n_act;
   int g = 0;
@@ -191,7 +191,7 @@ __device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtr
   } else {
     bin = i_pp;
   }
-  const double phi = point ? 0.0 : healpix_phi(p.n_side, ring, s.j[jj]);
+  const double phi = point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs);
   const double phase_shift = phi / kTwoPi;
   double ppt;
   if (n_gl > 0) {
@@ -203,7 +203,9 @@ __device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtr
     ppt = bin * (1.0 / p.n_bins);
     wgl = 1.0;
   }
-  double patch = fmod(ppt + phase_shift + 1., 1.);
+  // fmod(x, 1) of x = ppt + phase_shift + 1 in [1, 3): x - floor(x) is the same exact value
+  const double xph = ppt + phase_shift + 1.;
+  double patch = xph - floor(xph);
   if (patch < s.P[0]) patch += 1.;
   double af;
   const int i = vhunt(s.P, p.n_fine + 1, patch, af);
@@ -248,6 +250,7 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 320, MINB) integrand_nsx_ker
     const bool point = sp.kind == 1;
     const int n_act = tile_prologue(a, p, sp, tile, s, s_g, s_int, true);
     if (n_act == 0) continue;
+    const RingPhi rp = point ? RingPhi{0.0, 0.0} : healpix_ring_phi(p.n_side, tile.ring);
 
     // ---- step 5: (logT, logg) pre-reduction of the NSX table into S[E][mu]
     if (tid == 0) {
@@ -345,7 +348,7 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 320, MINB) integrand_nsx_ker
       const int q = q0 + tid;
       if (q < n_pts) {
         double wgl, z = 0, mu = 0;
-        const double flux = phase_point(p, s, tile.ring, point, n_act, q, bin, wgl, z, mu);
+        const double flux = phase_point(p, s, rp, point, n_act, q, bin, wgl, z, mu);
         if (flux != 0.0) {
           vis = true;
           if (mu < mu_min) mu = mu_min;
@@ -607,6 +610,7 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
     const bool point = sp.kind == 1;
     const int n_act = tile_prologue(a, p, sp, tile, s, s_g, s_int, true);
     if (n_act == 0) continue;
+    const RingPhi rp = point ? RingPhi{0.0, 0.0} : healpix_ring_phi(p.n_side, tile.ring);
 
     // ---- (logT, logg) pre-reduction of the NSX table into S[E][mu] (row stride ldS)
     if (tid == 0) {
@@ -731,7 +735,7 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
       const int q = q0 + tid;
       if (q < n_pts) {
         double wgl, z = 0, mu = 0;
-        const double flux = phase_point(p, s, tile.ring, point, n_act, q, bin, wgl, z, mu);
+        const double flux = phase_point(p, s, rp, point, n_act, q, bin, wgl, z, mu);
         if (flux != 0.0) {
           vis = true;
           if (mu < mu_min) mu = mu_min;
@@ -855,6 +859,7 @@ __global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
     const bool point = sp.kind == 1;
     const int n_act = tile_prologue(a, p, sp, tile, s, s_g, s_int, false);
     if (n_act == 0) continue;
+    const RingPhi rp = point ? RingPhi{0.0, 0.0} : healpix_ring_phi(p.n_side, tile.ring);
 
     const DevGrid& G = p.grid;
     const int n_e = G.n_e;
@@ -887,7 +892,7 @@ __global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
       const int q = q0 + tid;
       if (q < n_pts) {
         double wgl, z = 0, mu = 0;
-        const double flux = phase_point(p, s, tile.ring, point, n_act, q, bin, wgl, z, mu);
+        const double flux = phase_point(p, s, rp, point, n_act, q, bin, wgl, z, mu);
         if (flux != 0.0) {
           vis = true;
           c = flux * wgl;
