@@ -411,6 +411,10 @@ def main():
                 "convention": "80 FLOP per (element, bin, GL node, energy) regardless of visibility + per integrated "
                               "ring 120 per fine phase + 2*taps*166*67 slice",
                 "visible_points_per_launch": points, "evaluations_per_launch": evals,
+                "note": "the convention counts 80 FLOP per evaluation; the kernel contracts mu once per slice row "
+                        "and builds each cubic once per cell per phase point, so it executes fewer operations per "
+                        "evaluation and frac can exceed 1; its hardware bound is instruction issue (83.5 % of issue "
+                        "slots, profiles/integrand_nsx_cell_96profiles.md)",
             },
             "phases_ms": {"clear_plan": float(ph[0]), "integrand": float(ph[1]), "fold": float(ph[2])},
             "plain": {"value": plain_value, "unit": "profiles/s", "profiles": n_plain,
