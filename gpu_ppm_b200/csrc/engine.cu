@@ -907,7 +907,8 @@ void Engine::profile_batch(int n, const ppm_params* ps, double* flux, double* co
 
 IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max, int maxe_max,
                                     int bins_max) {
-  // home-cell NSX kernel: cpl cells per lane, 32 cpl per warp, warp sets up to 512 threads
+  // home-cell NSX kernel: cpl cells per lane (the last (cpl + 3) / cpl lanes of a warp
+  // only supply slice rows), warp sets up to 512 threads
   const int span_max = cells_max - 1;
   const int maxe_t = maxe_max <= 4 ? 4 : (maxe_max <= 8 ? 8 : 16);
   if (nsx_kernel && tune.kernel == 0 && maxe_max >= 1 && maxe_max <= 16 && span_max <= 16 * 32 && nsx.nmu < 4096 &&
@@ -917,8 +918,9 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
     const int cmax = maxe_t == 4 ? 3 : (maxe_t == 8 ? 2 : 1);
     int cpl = 1;
     long best = -1;
+    auto cells_per_warp = [](int c) { return (32 - (c + 3) / c) * c; };  // lanes with home cells x c
     for (int c = 1; c <= cmax; ++c) {
-      const long w = (span_max + 32 * c - 1) / (32 * c);
+      const long w = (span_max + cells_per_warp(c) - 1) / cells_per_warp(c);
       if (w > 16) continue;
       const long cost = w * (20 * (c + 1) + 30 + 11L * maxe_t * c);
       if (best < 0 || cost < best) {
@@ -927,22 +929,24 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
       }
     }
     if (tune.cpl > 0) cpl = std::min(tune.cpl, cmax);
-    const int cell_warps = (span_max + 32 * cpl - 1) / (32 * cpl);
-    // default: about 256 threads (three CTAs of 80 registers per SM measured fastest)
-    int sets = std::min(16 / cell_warps, tune.sets > 0 ? tune.sets : std::max(1, 8 / cell_warps));
-    IntegrandShape s;
-    for (;;) {
-      const int nt = 32 * cell_warps * sets;
-      s = make_shape(true, nt, 1, 1, tune.chunk, nf_max, lens.n_cp, lens.n_ca, nsx.nE, nsx.nmu, cells_max, true);
-      if (s.total <= 200 * 1024 || sets == 1) break;
-      --sets;
+    const int cell_warps = (span_max + cells_per_warp(cpl) - 1) / cells_per_warp(cpl);
+    if (best >= 0 && cell_warps <= 16) {
+      // default: about 256 threads (three CTAs of 80 registers per SM measured fastest)
+      int sets = std::min(16 / cell_warps, tune.sets > 0 ? tune.sets : std::max(1, 8 / cell_warps));
+      IntegrandShape s;
+      for (;;) {
+        const int nt = 32 * cell_warps * sets;
+        s = make_shape(true, nt, 1, 1, tune.chunk, nf_max, lens.n_cp, lens.n_ca, nsx.nE, nsx.nmu, cells_max, true);
+        if (s.total <= 200 * 1024 || sets == 1) break;
+        --sets;
+      }
+      s.bb_fp64 = 0;
+      s.cell_warps = cell_warps;
+      s.cpl = cpl;
+      s.maxe_t = maxe_t;
+      s.minb = maxe_t <= 8 ? tune.minb : 1;
+      return s;
     }
-    s.bb_fp64 = 0;
-    s.cell_warps = cell_warps;
-    s.cpl = cpl;
-    s.maxe_t = maxe_t;
-    s.minb = maxe_t <= 8 ? tune.minb : 1;
-    return s;
   }
   int ne_t = 1;
   if (ne_max > 512)

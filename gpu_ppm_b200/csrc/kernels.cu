@@ -539,13 +539,12 @@ __device__ __forceinline__ float slice_dot(const float* S, int ldS, int k, int i
   return fmaf(w.w, row[3], fmaf(w.z, row[2], fmaf(w.y, row[1], w.x * row[0])));
 }
 
-// cubic through h0..h3 at stencil nodes 0..3, in the fraction of cell `off` (0, 1, 2)
-__device__ __forceinline__ float4 cubic_cell(float h0, float h1, float h2, float h3, int off) {
-  const float d1 = h1 - h0, d2 = h2 - 2.f * h1 + h0, d3 = h3 - 3.f * h2 + 3.f * h1 - h0;
-  const float c3 = d3 * (1.f / 6.f);
-  if (off == 1) return make_float4(h1, d1 + 0.5f * d2 - c3, 0.5f * d2, c3);
-  if (off == 0) return make_float4(h0, d1 - 0.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 - 0.5f * d3, c3);
-  return make_float4(h2, d1 + 1.5f * d2 + d3 * (1.f / 3.f), 0.5f * d2 + 0.5f * d3, c3);
+// Lanes of a warp that only supply slice rows to their neighbours (no home
+// cells): a lane needs rows up to C + 3 past its first, i.e. own rows of the
+// next (C + 3) / C lanes.
+template <int C>
+__host__ __device__ constexpr int halo_lanes() {
+  return (C + 3) / C;
 }
 
 // Slice rows seen by one lane for one point record.  The lane owns C
@@ -553,8 +552,7 @@ __device__ __forceinline__ float4 cubic_cell(float h0, float h1, float h2, float
 // needs the cubics of cells g .. g + C, i.e. rows g - 1 .. g + C + 2 of the
 // mu-contracted slice: window h[j] = row g - 1 + j, j = 0 .. C + 3.  The lane
 // contracts rows j < C itself; row j >= C is own row j mod C of lane
-// lane + j / C, or, past the end of the warp, one of the four rows after the
-// warp's last own row, which lanes 28..31 contract.
+// lane + j / C (the last halo_lanes<C>() lanes of the warp own no cells).
 // Sx points at slice row 0 of a slice with rows -2 .. nE + 1: rows -1 and nE
 // hold the cubic extrapolations of the first and last four rows, so that the
 // centred stencil of cell 0 (rows -1..2) and of cell nE - 2 (rows nE - 3..nE)
@@ -562,19 +560,31 @@ __device__ __forceinline__ float4 cubic_cell(float h0, float h1, float h2, float
 // rows -2 and nE + 1 repeat rows 0 and nE - 1, and window rows are clamped to
 // -2 .. nE + 1, so cells past either end see the end value H[0] / H[nE - 1].
 template <int C>
-__device__ __forceinline__ void lane_window(const float* Sx, int ldS, int nE, int lane, int g, int gw, int imu,
-                                            float4 w, float (&h)[C + 4]) {
+__device__ __forceinline__ void lane_window(const float* Sx, int ldS, int nE, int g, int imu, float4 w,
+                                            float (&h)[C + 4]) {
 #pragma unroll
   for (int j = 0; j < C; ++j) h[j] = slice_dot(Sx, ldS, min(max(g - 1 + j, -2), nE + 1), imu, w);
-  // rows gw + 32 C - 1 + m, m = 0..3 (gw = G0 + first cell of the warp)
-  float xr = 0.f;
-  if (lane >= 28) xr = slice_dot(Sx, ldS, min(max(gw + 32 * C - 1 + (lane - 28), -2), nE + 1), imu, w);
 #pragma unroll
-  for (int j = C; j < C + 4; ++j) {
-    const int q = j / C, jj = j - q * C;
-    const float own = __shfl_down_sync(0xffffffffu, h[jj], q);
-    const float extra = __shfl_sync(0xffffffffu, xr, (C * lane + j - 32 * C + 28) & 31);
-    h[j] = lane + q < 32 ? own : extra;
+  for (int j = C; j < C + 4; ++j) h[j] = __shfl_down_sync(0xffffffffu, h[j % C], j / C);
+}
+
+// Cubics of the C + 1 cells whose stencils are window rows i .. i + 3 (the
+// cell between rows i + 1 and i + 2), in the cell fraction t: the Newton form
+// about row i + 1 rewritten as q0 + t (q1 + t (q2 + t q3)), from forward
+// differences shared by neighbouring cells.
+template <int C>
+__device__ __forceinline__ void window_cubics(const float (&h)[C + 4], float4 (&Q)[C + 1]) {
+  float d1[C + 3], d2[C + 2], d3[C + 1];
+#pragma unroll
+  for (int j = 0; j < C + 3; ++j) d1[j] = h[j + 1] - h[j];
+#pragma unroll
+  for (int j = 0; j < C + 2; ++j) d2[j] = d1[j + 1] - d1[j];
+#pragma unroll
+  for (int j = 0; j < C + 1; ++j) d3[j] = d2[j + 1] - d2[j];
+#pragma unroll
+  for (int i = 0; i <= C; ++i) {
+    const float c3 = d3[i] * (1.f / 6.f);
+    Q[i] = make_float4(h[i + 1], d1[i] + 0.5f * d2[i] - c3, 0.5f * d2[i], c3);
   }
 }
 
@@ -594,8 +604,9 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
   const int nE = X.nE, nmu = X.nmu, ldS = S.ldS;
   const int lane = tid & 31, warp = tid >> 5;
   const int set = warp / S.cell_warps, n_sets = (nt >> 5) / S.cell_warps;
-  const int wc = (warp - set * S.cell_warps) * 32 * C;  // first cell of the warp
-  const int r0 = wc + C * lane;                         // first of the lane's C home cells
+  constexpr int kOwners = 32 - halo_lanes<C>();        // lanes with home cells
+  const int wc = (warp - set * S.cell_warps) * kOwners * C;  // first cell of the warp
+  const int r0 = wc + C * lane;                              // first of the lane's C home cells
   float4* rec = (float4*)s.batch;  // [nt][2]: {c, fP, bin | imu << 20, G0}, {mu weights}
 
   for (;;) {
@@ -693,8 +704,9 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
 #pragma unroll
     for (int i = 0; i < C; ++i) {
       const int rc = r0 + i;
-      e0[i] = rc < G.span ? G.cell_first[rc] : 0;
-      cnt[i] = rc < G.span ? min(G.cell_first[rc + 1] - e0[i], MAXE) : 0;
+      const bool own = lane < kOwners && rc < G.span;
+      e0[i] = own ? G.cell_first[rc] : 0;
+      cnt[i] = own ? min(G.cell_first[rc + 1] - e0[i], MAXE) : 0;
 #pragma unroll
       for (int k = 0; k < MAXE; ++k) {
         fEv[i][k] = k < cnt[i] ? G.fEs[e0[i] + k] : 0.f;
@@ -795,12 +807,14 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
         }
         const int g = __float_as_int(rA.w) + r0;  // first home cell of the lane for this point
         float h[C + 4];
-        lane_window<C>(Sx, ldS, nE, lane, g, __float_as_int(rA.w) + wc, (int)(packed >> 20), wA, h);
+        lane_window<C>(Sx, ldS, nE, g, (int)(packed >> 20), wA, h);
         float4 Q[C + 1];
+        if (cubicE) {
+          window_cubics<C>(h, Q);
+        } else {
 #pragma unroll
-        for (int i = 0; i <= C; ++i)
-          Q[i] = cubicE ? cubic_cell(h[i], h[i + 1], h[i + 2], h[i + 3], 1)
-                        : make_float4(h[i + 1], h[i + 2] - h[i + 1], 0.f, 0.f);
+          for (int i = 0; i <= C; ++i) Q[i] = make_float4(h[i + 1], h[i + 2] - h[i + 1], 0.f, 0.f);
+        }
         // cells past an end hold the end value: H[0] is h[i] there; H[nE - 1]
         // is h[i + 1], except where that window row is the extrapolated row nE
         if (__any_sync(0xffffffffu, g < 0 || g + C > nE - 2)) {
