@@ -588,6 +588,28 @@ __device__ __forceinline__ void window_cubics(const float (&h)[C + 4], float4 (&
   }
 }
 
+// Packed FP32 pairs (add / fma .f32x2, one instruction for two lanes of
+// arithmetic): two energy slots of one cell share the cubics' coefficients.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pk(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void upk(f32x2 v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
 template <int MAXE, int C, int NTMAX, int MINB>
 __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const KernelArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
@@ -698,9 +720,9 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
     // ---- deposit
     const DevGrid& G = p.grid;
     const int n_e = G.n_e;
-    // per home cell i of the lane: its energies (MAXE slots: fraction, partial sum)
+    // per home cell i of the lane: its energies, MAXE slots in pairs (fractions, partial sums)
     int e0[C], cnt[C];
-    float fEv[C][MAXE], acc[C][MAXE];
+    f32x2 fE2[C][MAXE / 2], acc2[C][MAXE / 2];
 #pragma unroll
     for (int i = 0; i < C; ++i) {
       const int rc = r0 + i;
@@ -708,9 +730,9 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
       e0[i] = own ? G.cell_first[rc] : 0;
       cnt[i] = own ? min(G.cell_first[rc + 1] - e0[i], MAXE) : 0;
 #pragma unroll
-      for (int k = 0; k < MAXE; ++k) {
-        fEv[i][k] = k < cnt[i] ? G.fEs[e0[i] + k] : 0.f;
-        acc[i][k] = 0.f;
+      for (int k = 0; k < MAXE / 2; ++k) {
+        fE2[i][k] = pk(2 * k < cnt[i] ? G.fEs[e0[i] + 2 * k] : 0.f, 2 * k + 1 < cnt[i] ? G.fEs[e0[i] + 2 * k + 1] : 0.f);
+        acc2[i][k] = pk(0.f, 0.f);
       }
     }
     const int mode = p.interp;
@@ -728,11 +750,14 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
       for (int i = 0; i < C; ++i)
 #pragma unroll
         for (int k = 0; k < MAXE; ++k) {
-          if (k < cnt[i] && acc[i][k] != 0.f) {
+          float lo, hi;
+          upk(acc2[i][k / 2], lo, hi);
+          const float v = (k & 1) ? hi : lo;
+          if (k < cnt[i] && v != 0.f) {
             const int e = G.perm[e0[i] + k];
-            atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)acc[i][k] * out_scale * G.invE[e]);
+            atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)v * out_scale * G.invE[e]);
           }
-          acc[i][k] = 0.f;
+          if (k & 1) acc2[i][k / 2] = pk(0.f, 0.f);
         }
     };
 
@@ -825,20 +850,31 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
             if (gi > nE - 2) Q[i] = make_float4(gi == nE ? h[i] : h[i + 1], 0.f, 0.f, 0.f);
           }
         }
-        const float cw = rA.x, fP = rA.y;
+        const f32x2 cw2 = pk(rA.x, rA.x), fP2 = pk(rA.y, rA.y), m1 = pk(-1.f, -1.f);
 #pragma unroll
-        for (int i = 0; i < C; ++i)
+        for (int i = 0; i < C; ++i) {
+          const f32x2 ax = pk(Q[i].x, Q[i].x), ay = pk(Q[i].y, Q[i].y), az = pk(Q[i].z, Q[i].z), aw = pk(Q[i].w, Q[i].w);
+          const f32x2 bx = pk(Q[i + 1].x, Q[i + 1].x), by = pk(Q[i + 1].y, Q[i + 1].y), bz = pk(Q[i + 1].z, Q[i + 1].z),
+                      bw = pk(Q[i + 1].w, Q[i + 1].w);
 #pragma unroll
-          for (int k = 0; k < MAXE; ++k) {
+          for (int k = 0; k < MAXE / 2; ++k) {
             // split coordinate t = fE + fP: cell i below 1, cell i + 1 at t - 1
             // above; both cubics are evaluated and the result selected
-            const float t = fEv[i][k] + fP, t1 = t - 1.f;
-            const float v0 = fmaf(fmaf(fmaf(Q[i].w, t, Q[i].z), t, Q[i].y), t, Q[i].x);
-            const float v1 = fmaf(fmaf(fmaf(Q[i + 1].w, t1, Q[i + 1].z), t1, Q[i + 1].y), t1, Q[i + 1].x);
-            float v = t >= 1.f ? v1 : v0;
-            if (sg) v = fmaxf(v, 0.f);
-            acc[i][k] = fmaf(cw, v, acc[i][k]);
+            const f32x2 t0 = add2(fE2[i][k], fP2), t1 = add2(t0, m1);
+            const f32x2 v0 = fma2(fma2(fma2(aw, t0, az), t0, ay), t0, ax);
+            const f32x2 v1 = fma2(fma2(fma2(bw, t1, bz), t1, by), t1, bx);
+            float ta, tb, a0, b0, a1, b1;
+            upk(t0, ta, tb);
+            upk(v0, a0, b0);
+            upk(v1, a1, b1);
+            float va = ta >= 1.f ? a1 : a0, vb = tb >= 1.f ? b1 : b0;
+            if (sg) {
+              va = fmaxf(va, 0.f);
+              vb = fmaxf(vb, 0.f);
+            }
+            acc2[i][k] = fma2(cw2, pk(va, vb), acc2[i][k]);
           }
+        }
       }
       // no barrier here: the next round writes records only after the barriers
       // of its compaction, which every warp reaches after this loop
