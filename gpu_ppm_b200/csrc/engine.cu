@@ -158,9 +158,11 @@ Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   PPM_CUDA(cudaSetDevice(cfg.device));
   PPM_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, cfg.device));
   PPM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-  // launch-shape overrides for experiments: PPM_PB, PPM_CHUNK, PPM_NE_T, PPM_MINB, PPM_KERNEL, PPM_SETS, PPM_CPL
+  // launch-shape overrides for experiments: PPM_PB, PPM_CHUNK, PPM_SMALL_CHUNK, PPM_NE_T, PPM_MINB, PPM_KERNEL,
+  // PPM_SETS, PPM_CPL
   if (const char* v = std::getenv("PPM_PB")) tune.pb = std::max(1, std::atoi(v));
   if (const char* v = std::getenv("PPM_CHUNK")) tune.chunk = std::max(32, std::atoi(v));
+  if (const char* v = std::getenv("PPM_SMALL_CHUNK")) tune.small_chunk = std::max(32, std::atoi(v));
   if (const char* v = std::getenv("PPM_NE_T")) tune.ne_t = std::atoi(v);
   if (const char* v = std::getenv("PPM_MINB")) tune.minb = std::max(1, std::min(2, std::atoi(v)));
   if (const char* v = std::getenv("PPM_KERNEL")) tune.kernel = std::atoi(v) ? 1 : 0;
@@ -636,7 +638,7 @@ void Engine::fill_profile(const ppm_params& p, DevProfile& d, long long flux_off
 // Converts and uploads n profiles, sizes the work queue and output pools, and
 // records the launch shapes; the batch owns all of its device memory.
 void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t copy_stream, int ring_begin,
-                         int ring_end) {
+                         int ring_end, int chunk_override) {
   if (n < 1) throw Error(PPM_E_INVALID, "empty batch");
   if (ring_begin > ring_end) throw Error(PPM_E_INVALID, "ring window with begin > end");
   if (!B.mem.stream) B.mem.cache = &block_cache;
@@ -663,7 +665,8 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
   for (int v = 0; v < 3; ++v)
     for (int i = 0; i < n; ++i)
       if (variant(ps[i]) == v) order.push_back(i);
-  const int chunk = tune.chunk;
+  const int chunk = chunk_override > 0 ? chunk_override : tune.chunk;
+  B.chunk = chunk;
   B.d_stats = (unsigned long long*)B.mem.alloc(sizeof(unsigned long long) * kStats * (size_t)n);
   std::vector<DevProfile> hp(n);
   long long cap[3] = {0, 0, 0};
@@ -778,7 +781,7 @@ void Engine::batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events) {
   PPM_CUDA(cudaMemsetAsync(B.d_flux, 0, sizeof(double) * (size_t)B.flux_off[n], st));
   PPM_CUDA(cudaMemsetAsync(B.d_stats, 0, sizeof(unsigned long long) * kStats * (size_t)n, st));
   PPM_CUDA(cudaMemsetAsync(B.d_ctrl, 0, sizeof(int) * 16, st));
-  for (const auto& G : B.groups) PPM_CUDA(launch_plan(B.d_prof + G.g0, G.g1 - G.g0, lens, G.args.queue, tune.chunk, st));
+  for (const auto& G : B.groups) PPM_CUDA(launch_plan(B.d_prof + G.g0, G.g1 - G.g0, lens, G.args.queue, B.chunk, st));
   if (events) PPM_CUDA(cudaEventRecord(events[1], st));
   for (const auto& G : B.groups) PPM_CUDA(launch_integrand(G.args, G.grid, st));
   if (events) PPM_CUDA(cudaEventRecord(events[2], st));
@@ -879,7 +882,7 @@ void Engine::profile(const ppm_params& p, double* flux, double* counts, ppm_resu
   std::lock_guard<std::mutex> lk(mu);
   if (counts && p.response < 0) throw Error(PPM_E_INVALID, "counts requested without a response");
   BatchImpl B;
-  batch_build(B, 1, &p);
+  batch_build(B, 1, &p, nullptr, 0, 1 << 30, plain_chunk());
   batch_enqueue(B, stream, nullptr);  // plain form: direct launches, no graph
   B.last_stream = stream;
   batch_collect(B, flux, counts, info, stream);
@@ -890,7 +893,7 @@ void Engine::profile_rings(const ppm_params& p, int ring_begin, int ring_end, do
   std::lock_guard<std::mutex> lk(mu);
   if (counts && p.response < 0) throw Error(PPM_E_INVALID, "counts requested without a response");
   BatchImpl B;
-  batch_build(B, 1, &p, nullptr, ring_begin, ring_end);
+  batch_build(B, 1, &p, nullptr, ring_begin, ring_end, plain_chunk());
   batch_enqueue(B, stream, nullptr);
   B.last_stream = stream;
   batch_collect(B, flux, counts, info, stream);

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <condition_variable>
 #include <deque>
@@ -128,6 +129,7 @@ struct BatchImpl {
   size_t h2d_bytes = 0;
   cudaGraphExec_t graph = nullptr;
   cudaStream_t last_stream = nullptr;
+  int chunk = 1024;                // candidate elements per tile of this batch
   long long* d_fit_off = nullptr;  // counts offset per profile (fit statistics)
   ppm_fit* d_fit = nullptr;
   BatchImpl() = default;
@@ -149,6 +151,7 @@ void split_grid(const std::vector<double>& E, double inv_dE, GridSplit& out);
 struct Tuning {
   int pb = 20;       // phase points per polynomial sub-batch (rounded to whole warps)
   int chunk = 1024;  // candidate elements per tile
+  int small_chunk = 32;  // candidate elements per tile of the one-profile calls (more tiles in flight)
   int ne_t = 0;      // energies per thread (0 = automatic)
   int minb = 2;      // CTAs per SM targeted by the register budget
   int kernel = 0;    // NSX integrand: 0 = home-cell kernel where the grid allows, 1 = pooled-polynomial kernel
@@ -182,8 +185,11 @@ class Engine {
   void profile(const ppm_params& p, double* flux, double* counts, ppm_result_info* info);
   void profile_batch(int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info);
   // ring_begin/ring_end: only HEALPix rings i in [ring_begin, ring_end) (point sources count as ring 0)
+  // chunk: candidate elements per tile (0 = the tuned batch value)
   void batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t copy_stream = nullptr, int ring_begin = 0,
-                   int ring_end = 1 << 30);
+                   int ring_end = 1 << 30, int chunk = 0);
+  // tile size of the one-profile calls: a single profile cannot fill the GPU with ring-sized tiles
+  int plain_chunk() const { return std::min(tune.chunk, tune.small_chunk); }
   size_t request_bytes(const ppm_params& p) const;
   void warm_tables(const ppm_params& p);
   void batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events);

@@ -17,6 +17,7 @@
 // on the stream by each call, and calls that overlap on the GPU race on it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -135,14 +136,15 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   DevProfile d;
   unsigned long long* stats = (unsigned long long*)(base + o_stats);
   fill_profile(p, d, 0, stats, (const double*)(base + o_ring), (const double*)(base + o_fine), g, ring_rows);
-  // work-queue bound (as in batch_build)
+  // work-queue bound (as in batch_build, with the one-profile tile size)
+  const int chunk = plain_chunk();
   long long cap = 0;
   for (int s = 0; s < p.n_spots; ++s) {
     const DevSpot& sp = d.spot[s];
     if (sp.kind == PPM_SPOT_POINT)
       cap += 1;
     else if (sp.i_hi >= sp.i_lo)
-      cap += (long long)(sp.i_hi - sp.i_lo + 1) * (2 + (4ll * N + tune.chunk - 1) / tune.chunk);
+      cap += (long long)(sp.i_hi - sp.i_lo + 1) * (2 + (4ll * N + chunk - 1) / chunk);
   }
   if (cap > tile_cap)
     throw Error(PPM_E_RANGE, "ppm_profile_noalloc: the profile needs up to " + std::to_string(cap) +
@@ -189,7 +191,7 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   ck(configure_integrand_smem(a.shape), "shared-memory attribute");
   const int occ = max_active_ctas(a.shape);
   if (occ < 1) throw Error(PPM_E_RANGE, "ppm_profile_noalloc: launch shape does not fit on an SM");
-  ck(launch_plan(a.profiles, 1, lens, q, tune.chunk, st), "plan launch");
+  ck(launch_plan(a.profiles, 1, lens, q, chunk, st), "plan launch");
   ck(launch_integrand(a, (int)std::min<long long>((long long)sm_count * occ, std::max(1ll, cap)), st),
      "integrand launch");
   if (counts_d) {

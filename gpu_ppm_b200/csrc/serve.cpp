@@ -12,6 +12,7 @@
 // finished; the scheduler then copies each request's results into its
 // caller-owned buffers and completes the ticket with its submit-to-finish
 // latency.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>

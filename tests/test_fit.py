@@ -67,11 +67,11 @@ def test_batch_and_plain_fit_match_oracle_statistics():
         else:
             assert fits[k]["loglike"] == pytest.approx(ll, rel=1e-10), k
         assert fits[k]["n_zero_model"] == int(np.sum(m <= 0)), k
-    # the plain form gives the same statistics (the flux pool's FP64 atomics may
-    # add in another order from call to call, so equal to 1e-12, not bitwise)
+    # the plain form gives the same statistics up to the FP32 partial sums of the
+    # flux, which a one-profile launch splits into finer ring tiles than a batch
     f0, info = e.profile_fit(plist[k0], oid)
-    assert f0["chi2"] == pytest.approx(fits[k0]["chi2"], rel=1e-12)
-    assert f0["loglike"] == pytest.approx(fits[k0]["loglike"], rel=1e-12)
+    assert f0["chi2"] == pytest.approx(fits[k0]["chi2"], rel=1e-6)
+    assert f0["loglike"] == pytest.approx(fits[k0]["loglike"], rel=1e-9)
     assert info.n_points > 0
     # a profile with another bin count is rejected
     p = synth.draw_prior(1, seed=6, lens_u=(0.3, 0.5), n_side=32, n_bins=32, energy_grid=g, response=r)[0][0]
