@@ -473,7 +473,7 @@ def random_walk_requests(n, seed, grids, synth, abi):
 
 def serving_bench(lens, nsx, synth, abi, Engine, device, rates=((2000.0, 800), (100.0, 200))):
     """Open-loop Poisson request streams through ppm_submit (continuous batching)."""
-    eng = Engine(device=device, n_streams=4)
+    eng = Engine(device=device, n_streams=2)
     eng.load_lensing(lens)
     eng.load_nsx(nsx)
     grids = {}

@@ -149,7 +149,7 @@ void HostBuffer::release() {
 
 Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   if (cfg.memory_budget <= 0) cfg.memory_budget = 64ll << 30;
-  if (cfg.n_streams <= 0) cfg.n_streams = 4;
+  if (cfg.n_streams <= 0) cfg.n_streams = 2;
   if (cfg.max_batch <= 0) cfg.max_batch = 1 << 16;
   block_cache.set_limit((size_t)cfg.memory_budget);
   int n_dev = 0;
@@ -665,12 +665,12 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
   for (int v = 0; v < 3; ++v)
     for (int i = 0; i < n; ++i)
       if (variant(ps[i]) == v) order.push_back(i);
-  const int chunk = chunk_override > 0 ? chunk_override : tune.chunk;
-  B.chunk = chunk;
   B.d_stats = (unsigned long long*)B.mem.alloc(sizeof(unsigned long long) * kStats * (size_t)n);
   std::vector<DevProfile> hp(n);
   long long cap[3] = {0, 0, 0};
   int start[4] = {0, 0, 0, 0};
+  double work = 0;     // phase points of the batch, estimated from the spots' areas
+  long long pts_max = 1;  // phase points per element, largest profile
   for (int k = 0; k < n; ++k) {
     const int i = order[k];
     to_device(ps[i], hp[k], B.flux_off[i], B.d_stats + (size_t)kStats * i);
@@ -686,6 +686,14 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
         sp.i_hi = std::min(sp.i_hi, ring_end - 1);
       }
     }
+    const long long pts = (long long)ps[i].n_bins * std::max(1, ps[i].n_gl);
+    pts_max = std::max(pts_max, pts);
+    work += spot_elements(ps[i]) * (double)pts;
+  }
+  const int chunk = chunk_override > 0 ? chunk_override : tile_chunk(work, pts_max);
+  B.chunk = chunk;
+  for (int k = 0; k < n; ++k) {
+    const int i = order[k];
     const int v = variant(ps[i]);
     for (int s = 0; s < ps[i].n_spots; ++s) {
       const DevSpot& sp = hp[k].spot[s];
@@ -882,10 +890,33 @@ void Engine::profile(const ppm_params& p, double* flux, double* counts, ppm_resu
   std::lock_guard<std::mutex> lk(mu);
   if (counts && p.response < 0) throw Error(PPM_E_INVALID, "counts requested without a response");
   BatchImpl B;
-  batch_build(B, 1, &p, nullptr, 0, 1 << 30, plain_chunk());
+  batch_build(B, 1, &p);
   batch_enqueue(B, stream, nullptr);  // plain form: direct launches, no graph
   B.last_stream = stream;
   batch_collect(B, flux, counts, info, stream);
+}
+
+// HEALPix elements in a profile's spots (disk 1 areas over the element area,
+// one per point source): the size of its share of a batch's work.
+double Engine::spot_elements(const ppm_params& p) {
+  double e = 0;
+  for (int s = 0; s < p.n_spots; ++s) {
+    const ppm_spot& sp = p.spots[s];
+    e += sp.kind == PPM_SPOT_POINT ? 1.0
+                                   : 6.0 * p.n_side * (double)p.n_side * (1.0 - std::cos(std::min(std::fabs(sp.angrad1), pi)));
+  }
+  return e;
+}
+
+// Candidate elements per work tile: the tuned size unless one tile (up to
+// `chunk` elements x pts_max phase points) would exceed 1/8 of a CTA slot's
+// share of the batch's work, then halved down to small_chunk, so that small
+// batches, mixed served batches and single profiles end without a long tail.
+int Engine::tile_chunk(double work, long long pts_max) const {
+  const double share = work / (8.0 * sm_count * 3);
+  int c = tune.chunk;
+  while (c > tune.small_chunk && (double)c * pts_max > share) c >>= 1;
+  return std::max(c, std::min(tune.chunk, tune.small_chunk));
 }
 
 void Engine::profile_rings(const ppm_params& p, int ring_begin, int ring_end, double* flux, double* counts,
@@ -893,7 +924,7 @@ void Engine::profile_rings(const ppm_params& p, int ring_begin, int ring_end, do
   std::lock_guard<std::mutex> lk(mu);
   if (counts && p.response < 0) throw Error(PPM_E_INVALID, "counts requested without a response");
   BatchImpl B;
-  batch_build(B, 1, &p, nullptr, ring_begin, ring_end, plain_chunk());
+  batch_build(B, 1, &p, nullptr, ring_begin, ring_end);
   batch_enqueue(B, stream, nullptr);
   B.last_stream = stream;
   batch_collect(B, flux, counts, info, stream);

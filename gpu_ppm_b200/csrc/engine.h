@@ -151,7 +151,7 @@ void split_grid(const std::vector<double>& E, double inv_dE, GridSplit& out);
 struct Tuning {
   int pb = 20;       // phase points per polynomial sub-batch (rounded to whole warps)
   int chunk = 1024;  // candidate elements per tile
-  int small_chunk = 32;  // candidate elements per tile of the one-profile calls (more tiles in flight)
+  int small_chunk = 32;  // smallest tile: batches with little work split rings down to this size
   int ne_t = 0;      // energies per thread (0 = automatic)
   int minb = 2;      // CTAs per SM targeted by the register budget
   int kernel = 0;    // NSX integrand: 0 = home-cell kernel where the grid allows, 1 = pooled-polynomial kernel
@@ -188,8 +188,9 @@ class Engine {
   // chunk: candidate elements per tile (0 = the tuned batch value)
   void batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t copy_stream = nullptr, int ring_begin = 0,
                    int ring_end = 1 << 30, int chunk = 0);
-  // tile size of the one-profile calls: a single profile cannot fill the GPU with ring-sized tiles
-  int plain_chunk() const { return std::min(tune.chunk, tune.small_chunk); }
+  // candidate elements per tile for a batch of about `work` phase points, pts_max per element
+  int tile_chunk(double work, long long pts_max) const;
+  static double spot_elements(const ppm_params& p);
   size_t request_bytes(const ppm_params& p) const;
   void warm_tables(const ppm_params& p);
   void batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events);

@@ -138,7 +138,7 @@ void Engine::batch_fit(BatchImpl& B, int obs, ppm_fit* out, cudaStream_t st) {
 void Engine::profile_fit(const ppm_params& p, int obs, ppm_fit* out, ppm_result_info* info) {
   std::lock_guard<std::mutex> lk(mu);
   BatchImpl B;
-  batch_build(B, 1, &p, nullptr, 0, 1 << 30, plain_chunk());
+  batch_build(B, 1, &p);
   batch_enqueue(B, stream, nullptr);
   B.last_stream = stream;
   batch_fit(B, obs, out, stream);

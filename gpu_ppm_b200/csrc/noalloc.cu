@@ -136,8 +136,9 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   DevProfile d;
   unsigned long long* stats = (unsigned long long*)(base + o_stats);
   fill_profile(p, d, 0, stats, (const double*)(base + o_ring), (const double*)(base + o_fine), g, ring_rows);
-  // work-queue bound (as in batch_build, with the one-profile tile size)
-  const int chunk = plain_chunk();
+  // work-queue bound (as in batch_build, with its tile size)
+  const long long pts = (long long)p.n_bins * std::max(1, p.n_gl);
+  const int chunk = tile_chunk(spot_elements(p) * (double)pts, pts);
   long long cap = 0;
   for (int s = 0; s < p.n_spots; ++s) {
     const DevSpot& sp = d.spot[s];

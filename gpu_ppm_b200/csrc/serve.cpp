@@ -271,7 +271,8 @@ size_t Engine::request_bytes(const ppm_params& p) const {
   if (p.response >= 0) b += sizeof(double) * (size_t)resps[p.response].n_ch * p.n_bins;
   for (int s = 0; s < p.n_spots; ++s) {
     const long long rings = p.spots[s].kind == PPM_SPOT_POINT ? 1 : 4ll * p.n_side - 1;
-    b += sizeof(Tile) * (size_t)rings * (2 + (4 * (size_t)p.n_side + tune.chunk - 1) / tune.chunk);
+    const size_t chunk = (size_t)std::min(tune.chunk, tune.small_chunk);  // the finest tiles a batch may use
+    b += sizeof(Tile) * (size_t)rings * (2 + (4 * (size_t)p.n_side + chunk - 1) / chunk);
   }
   return b + sizeof(DevProfile) + sizeof(unsigned long long) * kStats + 4096;
 }

@@ -233,13 +233,25 @@ def test_table_edges_and_even_mu(monkeypatch, kernel):
         e.close()
 
 
-def test_ring_windows_sum_to_full_profile(eng_v171019):
+def test_ring_windows_sum_to_full_profile(monkeypatch):
     """ppm_profile_rings / ppm_batch_create_rings over a 3-way ring partition:
     each window matches the oracle on the same rings and the windows sum to the
-    whole profile (FP64 fold, 1e-12); a point-source spot belongs to ring 0."""
+    whole profile (FP64 fold, 1e-12, with one fixed tile size so that every
+    call groups the FP32 partial sums alike); a point-source spot belongs to ring 0."""
     from gpu_ppm_b200 import dist as pdist
 
-    g, r, E, rsp = eng_v171019.cfg2
+    monkeypatch.setenv("PPM_CHUNK", "64")
+    monkeypatch.setenv("PPM_SMALL_CHUNK", "64")
+    lens, nsx = synth.lensing("std"), synth.nsx("v171019", seed=0)
+    eng = Engine()
+    eng.load_lensing(lens)
+    eng.load_nsx(nsx)
+    E = synth.energy_grid(300, 0.2, 12.0)
+    g = eng.add_energy_grid(E)
+    rsp = synth.response(300, 1000, E, seed=0)
+    r = eng.add_response(g, rsp)
+    eng.ora = oracle.Oracle(lens, nsx)
+    eng_v171019 = eng
     p = synth.config2_params(g, r, n_side=48, n_bins=16, fold=_abi.FOLD_FP64)
     full_f, full_c, _ = eng_v171019.profile(p)
     wins = pdist.ring_partition(pdist.ring_costs(p), 3)
@@ -269,3 +281,4 @@ def test_ring_windows_sum_to_full_profile(eng_v171019):
     f0, _, _ = eng_v171019.profile_rings(q, 0, 1)
     f1, _, i1 = eng_v171019.profile_rings(q, 1, 4 * 48)
     assert np.array_equal(f0, pf) and not f1.any() and i1.n_points == 0
+    eng.close()

@@ -1,8 +1,8 @@
 """Serving (continuous batching): requests of mixed sizes submitted while
-others are in flight give the same results as the same profile run alone in a
-batch, and every ticket reports a latency.  Tolerance: 1e-9 relative (FP64
-atomic accumulation order is the only difference between a request alone and
-in a mix)."""
+others are in flight give the same results as the same profile run alone, and
+every ticket reports a latency.  Tolerance: 1e-5 relative (entries below 1e-6
+of the maximum by absolute error): a batch with few rings splits them into
+finer work tiles, which group the FP32 partial sums differently."""
 import numpy as np
 import pytest
 
@@ -58,9 +58,9 @@ def test_mix_equals_alone_and_latency_reported(served):
         assert info.status == 0
         assert e.latency_us(t) > 0
     for p, (flux, counts) in zip(reqs, bufs):
-        f1, c1, _ = e.profile_batch([p])
-        assert max_rel(flux, f1[0]) < 1e-9
-        assert max_rel(counts, c1[0]) < 1e-9
+        f1, c1, _ = e.profile(p)
+        assert max_rel(flux, f1) < 1e-5
+        assert max_rel(counts, c1) < 1e-5
 
 
 def test_invalid_request_rejected_at_submit(served):
