@@ -414,7 +414,7 @@ def main():
                 "visible_points_per_launch": points, "evaluations_per_launch": evals,
                 "note": "the convention counts 80 FLOP per evaluation; the kernel contracts mu once per slice row "
                         "and builds each cubic once per cell per phase point, so it executes fewer operations per "
-                        "evaluation and frac can exceed 1; its hardware bound is instruction issue (83.5 % of issue "
+                        "evaluation and frac can exceed 1; its hardware bound is instruction issue with the FMA and ALU pipes (74 % of issue "
                         "slots, profiles/integrand_nsx_cell_96profiles.md)",
             },
             "phases_ms": {"clear_plan": float(ph[0]), "integrand": float(ph[1]), "fold": float(ph[2])},
