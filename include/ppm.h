@@ -259,12 +259,15 @@ int ppm_batch_kernel_count(ppm_engine* e, ppm_batch* b, int32_t* n);
  * Calls share the array, so calls that overlap on the GPU race. */
 int ppm_profile_noalloc(ppm_engine* e, const ppm_params* p, double* flux_device, double* counts_device, void* stream);
 
-/* Autotuner: times candidate launch shapes of the integrand — phase points per
- * polynomial sub-batch, candidate elements per work tile (ring granularity),
- * CTAs per SM the register budget targets, energies per thread — on the given
- * sample profiles by coordinate descent with CUDA events, keeps the fastest
- * for every later launch, and writes a one-line-per-candidate report
- * (truncated to report_len; report may be NULL). */
+/* Autotuner: times candidate launch shapes of the integrand — candidate
+ * elements per work tile (ring granularity), CTAs per SM the register budget
+ * targets, the NSX kernel (home-cell or pooled-polynomial) with its energy
+ * cells per lane and warp sets per CTA, or phase points per polynomial
+ * sub-batch and energies per thread — on the given sample profiles by
+ * coordinate descent with CUDA events, keeps the fastest for every later
+ * launch, and writes a one-line-per-candidate report (truncated to
+ * report_len; report may be NULL).  No counterpart in the reference, whose
+ * launch shape is fixed (one CTA per ring, gpu/devarshi24st_gpu.cu:460-463). */
 int ppm_engine_autotune(ppm_engine* e, int32_t n, const ppm_params* sample, char* report, int32_t report_len);
 
 /* ---- fit statistics (sampler likelihood) ------------------------------------ */
