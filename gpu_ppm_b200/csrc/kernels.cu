@@ -11,12 +11,17 @@
 //   4. gap fill / wrap                    cpu/devarshi24st_cpu.cpp:195-212
 //   5. NSX (logT, logg) slice pre-reduced into shared memory (FP32)
 //                                         gpu/devarshi24st_gpu.cu:323-351
-//   6. deposit: batches of phase points (FP64 phase, hunt, lerps); for each
-//      point the mu-contracted slice is turned into per-cell cubic
-//      polynomials in log(E/kT); every thread owns fixed energies and keeps
-//      per-bin partial sums in registers (no per-element atomics); a bin's
-//      partial sums are flushed once into the FP64 flux pool
-//                                         cpu/devarshi24st_cpu.cpp:214-241
+//   6. deposit: rounds of phase points (FP64 phase, hunt, lerps, mu weights),
+//      visible ones compacted into records; per record the mu-contracted slice
+//      becomes per-cell cubic polynomials in log(E/kT), evaluated for the
+//      observed energies with per-bin partial sums in registers (no
+//      per-element atomics); a bin's partial sums are flushed once into the
+//      FP64 flux pool                     cpu/devarshi24st_cpu.cpp:214-241
+//      Home-cell kernel (default): each lane owns the energies of a few NSX
+//      cells and builds their cubics in registers from shuffled slice rows.
+//      Pooled-polynomial kernel (grids with > 16 energies in one cell): one
+//      warp per point writes the cubics to shared memory, one thread per
+//      energy reads its cell's cubic.
 #include <cstdio>
 
 #include "kernels.cuh"
