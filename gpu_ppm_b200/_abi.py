@@ -144,6 +144,9 @@ SIGNATURES = {
     "ppm_wait": (c_int32, [c_void_p, c_uint64, c_int32, POINTER(ResultInfo)]),
     "ppm_ticket_latency_us": (c_int32, [c_void_p, c_uint64, POINTER(c_double)]),
     "ppm_lensing_generate": (c_int32, [POINTER(LensingSpec), DP, DP, DP]),
+    "ppm_response_prepare": (c_int32, [c_int32, c_int32, DP, DP, DP, DP, DP, c_int32, DP, DP]),
+    "ppm_ism_inst_prepare": (c_int32, [c_char_p, c_char_p, c_char_p, c_int32, c_int32, c_int32, c_int32, c_int32,
+                                       c_char_p]),
     "ppm_write_counts": (c_int32, [c_char_p, c_int32, c_int32, DP, c_int32]),
     "ppm_write_row": (c_int32, [c_char_p, c_int32, DP, c_int32]),
     "ppm_last_error_string": (c_char_p, []),

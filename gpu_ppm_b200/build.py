@@ -12,7 +12,7 @@ LIB = os.path.join(OUT_DIR, "libppm_b200.so")
 RUN = os.path.join(OUT_DIR, "ppm_run")
 
 SOURCES = ["kernels.cu", "fold_tc.cu", "engine.cu", "noalloc.cu", "fit.cu", "capi.cpp", "serve.cpp", "lensgen.cpp",
-           "util.cpp"]
+           "response.cpp", "util.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

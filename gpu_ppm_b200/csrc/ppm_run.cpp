@@ -18,11 +18,22 @@
 //   ppm_run tinterp <scenario-file>
 //       lines: name N_fine N_pts obs_theta theta angrad interp_type (cpu/t_interp.cpp:20-32)
 //       output:  output/<name>_flux_gpu.txt, 256 rows x 1024 energies
+//   ppm_run ism_inst std|high|ultra
+//       c_ism_inst.py: reads ext/model_data/{nicer-rmf6s-teamonly-array50_full_matrix.txt,
+//       nicer-consim135p-teamonly-array50_arf.txt, interstellar_phot_frac.txt}, keeps
+//       energies [0, 1800) and channels [30, 300), 128 / 256 / 512 observed energies
+//       (c_ism_inst.py:5-26), writes tables/ism_inst/<setting>/{num,E_obs,rsp}.txt
+//   ppm_run ism_inst <rmf> <arf> <ism|-> <i_e_min> <i_e_max> <i_ch_min> <i_ch_max> <n_e_obs> <out_dir>
+//       the same with explicit files, ranges and output folder (no GPU needed)
 //
 // Errors are reported with the engine's status codes and messages; the
 // process exits non-zero instead of the reference's exit(EXIT_FAILURE).
+#include <sys/stat.h>
+
+#include <cerrno>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <fstream>
 #include <string>
 #include <vector>
@@ -69,10 +80,37 @@ ppm_nsx_desc v200804_axes() {
 
 int main(int argc, char** argv) {
   if (argc < 3) {
-    std::fprintf(stderr, "usage: %s devarshi|os1|tinterp <scenario-file>\n", argv[0]);
+    std::fprintf(stderr, "usage: %s devarshi|os1|tinterp <scenario-file>\n       %s ism_inst std|high|ultra\n",
+                 argv[0], argv[0]);
     return 2;
   }
   const std::string mode = argv[1];
+  if (mode == "ism_inst") {  // response preparation: host only
+    int rc;
+    if (argc == 3) {
+      const std::string setting = argv[2];
+      const int n_obs = setting == "ultra" ? 512 : (setting == "high" ? 256 : (setting == "std" ? 128 : 0));
+      if (!n_obs) {
+        std::fprintf(stderr, "ppm_run: unknown ism_inst setting %s\n", setting.c_str());
+        return 2;
+      }
+      const std::string out = "tables/ism_inst/" + setting;
+      for (const std::string d : {std::string("tables"), std::string("tables/ism_inst"), out})
+        if (::mkdir(d.c_str(), 0755) != 0 && errno != EEXIST) return fail(PPM_E_IO, ("creating " + d).c_str());
+      rc = ppm_ism_inst_prepare("ext/model_data/nicer-rmf6s-teamonly-array50_full_matrix.txt",
+                                "ext/model_data/nicer-consim135p-teamonly-array50_arf.txt",
+                                "ext/model_data/interstellar_phot_frac.txt", 0, 1800, 30, 300, n_obs, out.c_str());
+    } else if (argc == 11) {
+      const std::string ism = argv[4];
+      rc = ppm_ism_inst_prepare(argv[2], argv[3], ism == "-" ? nullptr : argv[4], std::atoi(argv[5]), std::atoi(argv[6]),
+                                std::atoi(argv[7]), std::atoi(argv[8]), std::atoi(argv[9]), argv[10]);
+    } else {
+      std::fprintf(stderr, "usage: %s ism_inst std|high|ultra\n       %s ism_inst <rmf> <arf> <ism|-> <i_e_min> "
+                           "<i_e_max> <i_ch_min> <i_ch_max> <n_e_obs> <out_dir>\n", argv[0], argv[0]);
+      return 2;
+    }
+    return rc ? fail(rc, "response preparation") : 0;
+  }
   std::ifstream in(argv[2]);
   if (!in) {
     std::fprintf(stderr, "ppm_run: cannot open %s\n", argv[2]);

@@ -323,6 +323,26 @@ int ppm_ticket_latency_us(ppm_engine* e, uint64_t ticket, double* latency_us);
 int ppm_lensing_generate(const ppm_lensing_spec* spec, double* cos_alpha_of_u_cos_psi, double* lf_of_u_cos_psi,
                          double* cdt_over_R_of_u_cos_alpha);
 
+/* Instrument response on the integrand's energy grid, the computation of
+ * c_ism_inst.py:59-96: rsp[ch][i] = sum_j rmf[ch][j] area[j] ism[j] C[j][i],
+ * where C[j][i] integrates, over fine bin j = [e_lo[j], e_hi[j]], the
+ * not-a-knot cubic spline (scipy.interpolate.CubicSpline, the script's
+ * dependency) through the unit vector e_i on the knots e_obs[0..n_obs).
+ * rmf [n_ch][n_fine], area/e_lo/e_hi/ism [n_fine] (ism may be NULL: no
+ * interstellar factor), e_obs [n_obs] strictly increasing, rsp [n_ch][n_obs]. */
+int ppm_response_prepare(int32_t n_ch, int32_t n_fine, const double* rmf, const double* area, const double* e_lo,
+                         const double* e_hi, const double* ism, int32_t n_obs, const double* e_obs, double* rsp);
+/* c_ism_inst.py:30-101 as a library call: reads the RMF (last column of each
+ * line after 3 header lines, energy-major), the ARF (E_lo E_hi area after 3
+ * header lines) and, unless ism_path is NULL, the ISM table (columns 0 and 2:
+ * energy, transmission, splined at the bin middles and raised to the 5th
+ * power); keeps energies [i_e_min, i_e_max) and channels [i_ch_min, i_ch_max);
+ * builds E_obs = geomspace(E_lo[first], E_hi[last], n_e_obs); writes num.txt,
+ * E_obs.txt and rsp.txt (zeroing |v| < 1e-300) into out_dir, the folder that
+ * ppm_engine_load_ism_inst_dir reads. */
+int ppm_ism_inst_prepare(const char* rmf_path, const char* arf_path, const char* ism_path, int32_t i_e_min,
+                         int32_t i_e_max, int32_t i_ch_min, int32_t i_ch_max, int32_t n_e_obs, const char* out_dir);
+
 /* Writes counts[n_ch][n_bins] as n_ch lines of n_bins space-separated values,
  * the format of gpu/devarshi24st_gpu.cu:491-505 (precision 16) and
  * cpu/devarshi24st_cpu.cpp:246-260 (precision 10). */
