@@ -38,6 +38,7 @@ METRIC = "batched profiles/s vs plain at <=1e-4 rel err vs FP64; served p50/p99 
 FLOP_PER_EVAL = 80          # integrand FLOPs per (element, bin, GL node, energy), counted regardless of visibility
 FLOP_PER_FINE = 120         # fine-phase sweep, per integrated ring and fine phase
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+REL_FLOOR = 1e-6            # error metric of the parity tests
 
 
 def parse():
@@ -383,9 +384,13 @@ def main():
         served = serving_bench(lens, nsx, synth, _abi, Engine, local)
 
     # ---- CPU baseline (rank 0, N = 1)
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(plist, infos, E, lens, nsx, args)
+        cpu, sample, ref_flux = cpu_baseline(plist, infos, E, lens, nsx, args)
+        try:
+            parity = parity_vs_oracle(sample, ref_flux, plist, counts_host.numpy(), rsp)
+        except Exception as exc:  # reported in the line rather than losing the measurement
+            parity = {"error": f"{type(exc).__name__}: {exc}"}
 
     batch.close()
     if rank == 0:
@@ -430,6 +435,7 @@ def main():
                               "runs": served, "p50_ms": served[0]["p50_ms"], "p99_ms": served[0]["p99_ms"]}
         if cpu:
             line["cpu_baseline"] = cpu
+            line["parity"] = parity
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -523,13 +529,38 @@ def cpu_baseline(plist, infos, E, lens, nsx, args):
     sample = choose_sample(order, counts, args.cpu_seconds, cores)
     sample = sample[np.argsort(-ev[sample])]  # largest first on the dynamic work queue
     t0 = time.perf_counter()
-    ora.profile_batch([plist[i] for i in sample], E, n_threads=cores)
+    ref_flux, _ = ora.profile_batch([plist[i] for i in sample], E, n_threads=cores)
     dt = time.perf_counter() - t0
     rate = ev[sample].sum() / dt
     value = len(plist) / (ev.sum() / rate)
     return {"value": value, "unit": "profiles/s", "cores": cores, "kind": "port",
             "sample": f"{len(sample)} of the {len(plist)} profiles spread over the size range ({dt:.1f} s on "
-                      f"{cores} threads), extrapolated to the full batch by integrand evaluations"}
+                      f"{cores} threads), extrapolated to the full batch by integrand evaluations"}, sample, ref_flux
+
+
+def max_rel(a, ref, floor=REL_FLOOR):
+    """Largest relative error; entries below floor * max|ref| are normalised by max|ref|."""
+    scale = np.abs(ref).max()
+    if scale == 0:
+        return float(np.abs(a).max())
+    denom = np.where(np.abs(ref) >= floor * scale, np.abs(ref), scale)
+    return float((np.abs(a - ref) / denom).max())
+
+
+def parity_vs_oracle(sample, ref_flux, plist, counts, rsp):
+    """Error of the engine's counts (the e2e call's output) against the FP64 oracle's flux folded in FP64,
+    for the profiles the CPU baseline computed."""
+    import oracle
+
+    n_ch = rsp.shape[0]
+    off = np.cumsum([0] + [n_ch * p.n_bins for p in plist])
+    errs = []
+    for k, i in enumerate(sample):
+        got = counts[off[i]:off[i + 1]].reshape(n_ch, plist[i].n_bins)
+        errs.append(max_rel(got, oracle.fold(rsp, ref_flux[k], plist[i].exposure_s)))
+    return {"max_rel_err": max(errs), "median_rel_err": float(np.median(errs)), "profiles": len(errs),
+            "tolerance": 1e-4, "floor": REL_FLOOR,
+            "against": "FP64 oracle flux folded in FP64, the cpu_baseline sample; engine counts from the e2e call"}
 
 
 if __name__ == "__main__":
