@@ -7,15 +7,20 @@
 // stream.  Whenever a stream is free it admits the oldest waiting requests
 // whose device working set fits in what remains of the memory budget, builds
 // them into one batch with stream-ordered allocations and enqueues plan ->
-// integrand -> fold -> device-to-pinned copies; batches on different streams
-// overlap on the device.  A host callback after the copies marks the batch
-// finished; the scheduler then copies each request's results into its
-// caller-owned buffers and completes the ticket with its submit-to-finish
-// latency.
+// integrand -> fold -> device-to-pinned copies into a staging buffer of its
+// own; batches on different streams overlap on the device.  A host callback
+// after the copies marks the batch finished; the scheduler then frees its
+// stream and device memory at once and hands the staging buffer to a
+// completion thread, which copies each request's results into its
+// caller-owned buffers outside the lock and completes the tickets.  The
+// scheduler thus never waits on those host copies (page faults of fresh
+// caller buffers included) before it fills the freed stream again.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <list>
 #include <memory>
 #include <thread>
@@ -29,7 +34,22 @@ using Clock = std::chrono::steady_clock;
 
 namespace {
 constexpr int kMaxRequestsPerBatch = 256;
+constexpr size_t kMaxCompleting = 4;  // finished batches whose results are still being copied out
+
+HostBuffer take(HostBuffer& b) {
+  HostBuffer r = b;
+  b.ptr = nullptr;
+  b.cap = 0;
+  return r;
 }
+
+// staging sizes grow in powers of two (>= 1 MiB) so that a pooled buffer is rarely reallocated
+size_t staging_size(size_t bytes) {
+  size_t s = size_t(1) << 20;
+  while (s < bytes) s <<= 1;
+  return s;
+}
+}  // namespace
 
 struct Server {
   struct Request {
@@ -48,36 +68,40 @@ struct Server {
   };
   struct Slot {
     cudaStream_t stream = nullptr;
-    HostBuffer pinned;  // device-to-host staging of the slot's current batch
     bool busy = false;
   };
   struct InFlight {
     std::vector<Request> reqs;
-    std::unique_ptr<BatchImpl> B;
+    std::unique_ptr<BatchImpl> B;      // device side; freed as soon as the batch finished
+    std::vector<long long> flux_off, counts_off;
+    HostBuffer stage;                  // device-to-host staging of this batch, from the pool
     int slot = 0;
     size_t bytes = 0;
     std::atomic<bool> finished{false};
-    Clock::time_point t_done;
     Server* server = nullptr;
     int* ctrl = nullptr;                 // pinned copy of the queue control words
     unsigned long long* stats = nullptr; // pinned copy of the counters
     double* counts = nullptr;            // pinned copy of the counts pool
     double* flux = nullptr;              // pinned copy of the flux pool
+    bool want_flux = false;
   };
 
   Engine* eng = nullptr;
   std::mutex mu;
-  std::condition_variable cv;       // wakes the scheduler
-  std::condition_variable cv_done;  // wakes waiters
+  std::condition_variable cv;          // wakes the scheduler
+  std::condition_variable cv_complete; // wakes the completion thread
+  std::condition_variable cv_done;     // wakes waiters
   std::deque<Request> pending;
   std::vector<Slot> slots;
   std::list<std::unique_ptr<InFlight>> inflight;
+  std::deque<std::unique_ptr<InFlight>> completing;
+  std::vector<HostBuffer> stage_pool;
   std::unordered_map<uint64_t, Done> done;
   std::unordered_map<uint64_t, bool> known;
   size_t budget = 0, in_use = 0;
   uint64_t next_ticket = 1;
-  bool stop = false;
-  std::thread thread;
+  bool stop = false, scheduler_done = false;
+  std::thread thread, completer;
 
   explicit Server(Engine* e) : eng(e) {
     budget = (size_t)e->cfg.memory_budget;
@@ -93,6 +117,7 @@ struct Server {
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
     thread = std::thread([this] { loop(); });
+    completer = std::thread([this] { complete_loop(); });
   }
 
   ~Server() {
@@ -102,26 +127,33 @@ struct Server {
     }
     cv.notify_all();
     if (thread.joinable()) thread.join();
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      scheduler_done = true;
+    }
+    cv_complete.notify_all();
+    if (completer.joinable()) completer.join();
     for (auto& s : slots) {
       if (s.stream) {
         cudaStreamSynchronize(s.stream);
         cudaStreamDestroy(s.stream);
       }
-      s.pinned.release();
     }
+    for (auto& b : stage_pool) b.release();
   }
 
   static void CUDART_CB on_finished(void* arg) {
     InFlight* f = (InFlight*)arg;
-    f->t_done = Clock::now();
+    Server* s = f->server;  // f may be retired and destroyed as soon as it is marked finished
     f->finished.store(true);
     {
-      std::lock_guard<std::mutex> lk(f->server->mu);
+      std::lock_guard<std::mutex> lk(s->mu);
     }
-    f->server->cv.notify_all();
+    s->cv.notify_all();
   }
 
-  // Copies finished batches' results to their callers and completes the tickets.  Called with mu held.
+  // Frees the streams and device memory of finished batches and queues their
+  // results for the completion thread.  Called with mu held.
   void retire() {
     for (auto it = inflight.begin(); it != inflight.end();) {
       InFlight& f = **it;
@@ -129,34 +161,62 @@ struct Server {
         ++it;
         continue;
       }
-      const bool overflow = f.ctrl[2] || f.ctrl[5] || f.ctrl[8];
-      const BatchImpl& B = *f.B;
-      for (size_t i = 0; i < f.reqs.size(); ++i) {
-        const Request& r = f.reqs[i];
-        Done d;
-        d.latency_us = std::chrono::duration<double, std::micro>(f.t_done - r.t_submit).count();
-        if (overflow) {
-          d.status = PPM_E_RANGE;
-        } else {
-          if (r.flux) std::memcpy(r.flux, f.flux + B.flux_off[i], sizeof(double) * (size_t)r.n_flux);
-          if (r.counts && r.n_counts) std::memcpy(r.counts, f.counts + B.counts_off[i], sizeof(double) * (size_t)r.n_counts);
-          const unsigned long long* s = f.stats + (size_t)kStats * i;
-          d.info.n_active = (int64_t)(s[0] + s[5]);
-          d.info.n_rings = (int64_t)s[1];
-          d.info.n_dropped_rings = (int64_t)s[2];
-          d.info.n_points = (int64_t)s[3];
-          d.info.n_clamped = (int64_t)s[4];
-          d.info.n_active_integrated = (int64_t)s[0];
-        }
-        d.info.status = d.status;
-        done[r.ticket] = d;
-      }
-      slots[f.slot].busy = false;
-      in_use -= f.bytes;
+      f.flux_off = std::move(f.B->flux_off);
+      f.counts_off = std::move(f.B->counts_off);
       // stream-ordered frees of the batch's device memory on its own stream
       cudaSetDevice(eng->cfg.device);
+      f.B.reset();
+      slots[f.slot].busy = false;
+      in_use -= f.bytes;
+      completing.push_back(std::move(*it));
       it = inflight.erase(it);
+      cv_complete.notify_all();
+    }
+  }
+
+  // Copies one finished batch's results into the callers' buffers (no lock held).
+  static std::vector<std::pair<uint64_t, Done>> copy_out(const InFlight& f) {
+    std::vector<std::pair<uint64_t, Done>> out(f.reqs.size());
+    const bool overflow = f.ctrl[2] || f.ctrl[5] || f.ctrl[8];
+    for (size_t i = 0; i < f.reqs.size(); ++i) {
+      const Request& r = f.reqs[i];
+      Done& d = out[i].second;
+      out[i].first = r.ticket;
+      if (overflow) {
+        d.status = PPM_E_RANGE;
+      } else {
+        if (r.flux) std::memcpy(r.flux, f.flux + f.flux_off[i], sizeof(double) * (size_t)r.n_flux);
+        if (r.counts && r.n_counts) std::memcpy(r.counts, f.counts + f.counts_off[i], sizeof(double) * (size_t)r.n_counts);
+        const unsigned long long* s = f.stats + (size_t)kStats * i;
+        d.info.n_active = (int64_t)(s[0] + s[5]);
+        d.info.n_rings = (int64_t)s[1];
+        d.info.n_dropped_rings = (int64_t)s[2];
+        d.info.n_points = (int64_t)s[3];
+        d.info.n_clamped = (int64_t)s[4];
+        d.info.n_active_integrated = (int64_t)s[0];
+      }
+      d.info.status = d.status;
+    }
+    const Clock::time_point t = Clock::now();
+    for (size_t i = 0; i < f.reqs.size(); ++i)
+      out[i].second.latency_us = std::chrono::duration<double, std::micro>(t - f.reqs[i].t_submit).count();
+    return out;
+  }
+
+  void complete_loop() {
+    std::unique_lock<std::mutex> lk(mu);
+    while (true) {
+      cv_complete.wait(lk, [&] { return !completing.empty() || scheduler_done; });
+      if (completing.empty()) break;  // scheduler_done and nothing left
+      std::unique_ptr<InFlight> f = std::move(completing.front());
+      completing.pop_front();
+      lk.unlock();
+      auto out = copy_out(*f);
+      lk.lock();
+      for (auto& kv : out) done[kv.first] = kv.second;
+      stage_pool.push_back(take(f->stage));
       cv_done.notify_all();
+      cv.notify_all();  // the scheduler may be waiting for room in the completion queue
     }
   }
 
@@ -183,32 +243,38 @@ struct Server {
           free_slot = (int)k;
           break;
         }
-      if (pending.empty() || free_slot < 0) {
+      if (pending.empty() || free_slot < 0 || completing.size() >= kMaxCompleting) {
         cv.wait_for(lk, std::chrono::microseconds(200));
         continue;
       }
       // admit the oldest requests that fit the remaining budget
-      std::vector<Request> take;
+      std::vector<Request> take_reqs;
       size_t bytes = 0;
-      while (!pending.empty() && (int)take.size() < kMaxRequestsPerBatch &&
+      while (!pending.empty() && (int)take_reqs.size() < kMaxRequestsPerBatch &&
              in_use + bytes + pending.front().bytes <= budget) {
         bytes += pending.front().bytes;
-        take.push_back(pending.front());
+        take_reqs.push_back(pending.front());
         pending.pop_front();
       }
-      if (take.empty()) {  // waiting for memory to free up
+      if (take_reqs.empty()) {  // waiting for memory to free up
         cv.wait_for(lk, std::chrono::microseconds(200));
         continue;
       }
       Slot& slot = slots[free_slot];
       slot.busy = true;
       in_use += bytes;
-      lk.unlock();
       std::unique_ptr<InFlight> f(new InFlight());
       f->server = this;
       f->slot = free_slot;
       f->bytes = bytes;
-      f->reqs = std::move(take);
+      f->reqs = std::move(take_reqs);
+      if (!stage_pool.empty()) {  // the largest pooled staging buffer
+        auto big = std::max_element(stage_pool.begin(), stage_pool.end(),
+                                    [](const HostBuffer& a, const HostBuffer& b) { return a.cap < b.cap; });
+        f->stage = take(*big);
+        stage_pool.erase(big);
+      }
+      lk.unlock();
       int err = PPM_OK;
       try {
         launch(*f, slot);
@@ -219,6 +285,7 @@ struct Server {
       if (err != PPM_OK) {
         slot.busy = false;
         in_use -= bytes;
+        stage_pool.push_back(take(f->stage));
         fail(f->reqs, err);
         continue;
       }
@@ -240,12 +307,12 @@ struct Server {
     }
     // device -> pinned staging
     const size_t n_counts = (size_t)B.counts_off[n], n_flux = (size_t)B.flux_off[n];
-    bool want_flux = false;
-    for (auto& r : f.reqs) want_flux |= r.flux != nullptr;
+    f.want_flux = false;
+    for (auto& r : f.reqs) f.want_flux |= r.flux != nullptr;
     const size_t bytes = 64 + sizeof(unsigned long long) * kStats * n + sizeof(double) * n_counts +
-                         (want_flux ? sizeof(double) * n_flux : 0) + 256;
-    slot.pinned.reserve(bytes);
-    unsigned char* h = (unsigned char*)slot.pinned.ptr;
+                         (f.want_flux ? sizeof(double) * n_flux : 0) + 256;
+    f.stage.reserve(staging_size(bytes));
+    unsigned char* h = (unsigned char*)f.stage.ptr;
     f.ctrl = (int*)h;
     f.stats = (unsigned long long*)(h + 64);
     f.counts = (double*)(h + 64 + sizeof(unsigned long long) * kStats * n);
@@ -259,7 +326,7 @@ struct Server {
     if (n_counts)
       ck(cudaMemcpyAsync(f.counts, B.d_counts, sizeof(double) * n_counts, cudaMemcpyDeviceToHost, slot.stream),
          "serve copy");
-    if (want_flux)
+    if (f.want_flux)
       ck(cudaMemcpyAsync(f.flux, B.d_flux, sizeof(double) * n_flux, cudaMemcpyDeviceToHost, slot.stream), "serve copy");
     ck(cudaLaunchHostFunc(slot.stream, on_finished, &f), "serve callback");
   }
@@ -286,6 +353,7 @@ void Engine::warm_tables(const ppm_params& p) {
 }
 
 uint64_t Engine::submit(const ppm_params& p, double* flux, double* counts) {
+  const Clock::time_point t_entry = Clock::now();  // latency counts any wait for the engine lock
   {
     std::lock_guard<std::mutex> lk(mu);
     validate(p);
@@ -303,7 +371,7 @@ uint64_t Engine::submit(const ppm_params& p, double* flux, double* counts) {
   r.n_counts = p.response >= 0 ? (long long)resps[p.response].n_ch * p.n_bins : 0;
   r.bytes = request_bytes(p);
   if (r.bytes > server->budget) throw Error(PPM_E_OOM, "request larger than the serving memory budget");
-  r.t_submit = Clock::now();
+  r.t_submit = t_entry;
   {
     std::lock_guard<std::mutex> lk(server->mu);
     r.ticket = server->next_ticket++;

@@ -313,7 +313,8 @@ int ppm_submit(ppm_engine* e, const ppm_params* p, double* flux, double* counts,
 int ppm_poll(ppm_engine* e, uint64_t ticket, int32_t* done);
 /* Waits at most timeout_ms (negative: no limit) for a ticket. */
 int ppm_wait(ppm_engine* e, uint64_t ticket, int32_t timeout_ms, ppm_result_info* info);
-/* Submit-to-completion latency of a finished ticket, in microseconds. */
+/* Latency of a finished ticket, in microseconds: from the entry of ppm_submit
+ * to the moment its results are in the caller's buffers (ppm_wait can return). */
 int ppm_ticket_latency_us(ppm_engine* e, uint64_t ticket, double* latency_us);
 
 /* ---- tables & files ----------------------------------------------------------- */
