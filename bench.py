@@ -510,6 +510,7 @@ def serving_bench(lens, nsx, synth, abi, Engine, device, rates=((2000.0, 800), (
         for t in tickets:
             eng.wait(t)
             lat.append(eng.latency_us(t) / 1000.0)
+            eng.release(t)
         t_all = time.perf_counter() - t0
         results.append({"offered_req_per_s": rate, "requests": n, "throughput_req_per_s": n / t_all,
                         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),

@@ -143,6 +143,7 @@ SIGNATURES = {
     "ppm_poll": (c_int32, [c_void_p, c_uint64, POINTER(c_int32)]),
     "ppm_wait": (c_int32, [c_void_p, c_uint64, c_int32, POINTER(ResultInfo)]),
     "ppm_ticket_latency_us": (c_int32, [c_void_p, c_uint64, POINTER(c_double)]),
+    "ppm_ticket_release": (c_int32, [c_void_p, c_uint64]),
     "ppm_lensing_generate": (c_int32, [POINTER(LensingSpec), DP, DP, DP]),
     "ppm_response_prepare": (c_int32, [c_int32, c_int32, DP, DP, DP, DP, DP, c_int32, DP, DP]),
     "ppm_ism_inst_prepare": (c_int32, [c_char_p, c_char_p, c_char_p, c_int32, c_int32, c_int32, c_int32, c_int32,

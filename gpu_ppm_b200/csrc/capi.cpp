@@ -375,4 +375,8 @@ int ppm_ticket_latency_us(ppm_engine* e, uint64_t ticket, double* us) {
   });
 }
 
+int ppm_ticket_release(ppm_engine* e, uint64_t ticket) {
+  return guarded([&] { eng(e).release_ticket(ticket); });
+}
+
 }  // extern "C"

@@ -213,6 +213,7 @@ class Engine {
   int poll(uint64_t t);
   int wait(uint64_t t, int timeout_ms, ppm_result_info* info);
   double latency_us(uint64_t t);
+  void release_ticket(uint64_t t);
   void serve_shutdown();
 
   ppm_engine_config cfg;

@@ -412,6 +412,15 @@ double Engine::latency_us(uint64_t t) {
   return it->second.latency_us;
 }
 
+void Engine::release_ticket(uint64_t t) {
+  if (!server) throw Error(PPM_E_INVALID, "unknown ticket");
+  std::lock_guard<std::mutex> lk(server->mu);
+  if (!server->known.count(t)) throw Error(PPM_E_INVALID, "unknown ticket");
+  if (!server->done.count(t)) throw Error(PPM_E_STATE, "ticket not finished");
+  server->done.erase(t);
+  server->known.erase(t);
+}
+
 void Engine::serve_shutdown() {
   delete server;
   server = nullptr;

@@ -175,6 +175,10 @@ class Engine:
         check(lib().ppm_ticket_latency_us(self.h, ticket, ctypes.byref(v)))
         return v.value
 
+    def release(self, ticket):
+        """Forgets a finished ticket (ppm_ticket_release)."""
+        check(lib().ppm_ticket_release(self.h, ticket))
+
 
 class Batch:
     """Wraps ppm_batch: uploads/plans once; `launch(stream)` replays a CUDA graph

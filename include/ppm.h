@@ -316,6 +316,11 @@ int ppm_wait(ppm_engine* e, uint64_t ticket, int32_t timeout_ms, ppm_result_info
 /* Latency of a finished ticket, in microseconds: from the entry of ppm_submit
  * to the moment its results are in the caller's buffers (ppm_wait can return). */
 int ppm_ticket_latency_us(ppm_engine* e, uint64_t ticket, double* latency_us);
+/* Forgets a finished ticket (its status, info and latency); afterwards the
+ * ticket is unknown.  A long-running client releases each ticket once it has
+ * read it, so the engine's record of tickets stays bounded.  PPM_E_STATE if the
+ * ticket has not finished. */
+int ppm_ticket_release(ppm_engine* e, uint64_t ticket);
 
 /* ---- tables & files ----------------------------------------------------------- */
 

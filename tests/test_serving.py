@@ -57,6 +57,9 @@ def test_mix_equals_alone_and_latency_reported(served):
         info = e.wait(t, timeout_ms=120000)
         assert info.status == 0
         assert e.latency_us(t) > 0
+        e.release(t)
+        with pytest.raises(_abi.PpmError):  # a released ticket is unknown
+            e.poll(t)
     for p, (flux, counts) in zip(reqs, bufs):
         f1, c1, _ = e.profile(p)
         assert max_rel(flux, f1) < 1e-5
