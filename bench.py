@@ -202,18 +202,33 @@ def run_reference(args):
     value = args.n_profiles / (evals_full / rate)
     ms = 1000.0 * sum(t for t, _, _ in times) / len(times)
     sample_desc = (f"{int(np.mean(samples))} profiles per step spread over the active-element range of the "
-                   f"{args.n_profiles}-profile batch, {cores} threads; profiles/s extrapolated by integrand "
-                   "evaluations (element x bin x GL node x energy, elements estimated from spot areas)")
+                   f"{args.n_profiles}-profile batch, {cores} threads of {cpu_model()}; profiles/s extrapolated "
+                   "by integrand evaluations (element x bin x GL node x energy, elements estimated from spot areas)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "profiles/s", "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "batching prior, N_side 256, NSX 2l2c_le, 64 bins x 2 GL, 300 energies, "
                                "300-channel fold", "profiles": args.n_profiles},
-        "cpu_baseline": {"value": value, "unit": "profiles/s", "cores": cores, "kind": "port", "sample": sample_desc},
+        "cpu_baseline": {"value": value, "unit": "profiles/s", "cores": cores, "kind": "port", "cpu": cpu_model(),
+                         "sample": sample_desc},
         "e2e": {"value": value, "unit": "profiles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or the platform's processor string."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
 
 
 def choose_sample(order, counts, seconds, cores, offset=0, ns_per_eval=60.0):
@@ -534,9 +549,22 @@ def cpu_baseline(plist, infos, E, lens, nsx, args):
     dt = time.perf_counter() - t0
     rate = ev[sample].sum() / dt
     value = len(plist) / (ev.sum() / rate)
-    return {"value": value, "unit": "profiles/s", "cores": cores, "kind": "port",
+    # one core: the smallest profiles of the same sample, about 5 s of single-threaded work
+    one = []
+    budget = 5.0 * rate / cores
+    for i in sample[np.argsort(ev[sample])]:
+        if one and ev[np.array(one)].sum() + ev[i] > budget:
+            break
+        one.append(i)
+    t0 = time.perf_counter()
+    ora.profile_batch([plist[i] for i in one], E, n_threads=1)
+    dt1 = time.perf_counter() - t0
+    value_1 = len(plist) / (ev.sum() / (ev[np.array(one)].sum() / dt1))
+    return {"value": value, "unit": "profiles/s", "cores": cores, "kind": "port", "cpu": cpu_model(),
+            "value_1_core": value_1,
             "sample": f"{len(sample)} of the {len(plist)} profiles spread over the size range ({dt:.1f} s on "
-                      f"{cores} threads), extrapolated to the full batch by integrand evaluations"}, sample, ref_flux
+                      f"{cores} threads), extrapolated to the full batch by integrand evaluations; the one-core "
+                      f"figure from the {len(one)} smallest of them on one thread ({dt1:.1f} s)"}, sample, ref_flux
 
 
 def max_rel(a, ref, floor=REL_FLOOR):
