@@ -512,7 +512,7 @@ def serving_bench(lens, nsx, synth, abi, Engine, device, rates=((2000.0, 800), (
         reqs = random_walk_requests(n, 1000 + k, grids, synth, abi)
         rng = np.random.default_rng(k)
         t_arr = np.cumsum(rng.exponential(1.0 / rate, size=n))
-        bufs, tickets = [], []
+        bufs, tickets, lag, sub = [], [], [], []
         t0 = time.perf_counter()
         for p, ta in zip(reqs, t_arr):
             while time.perf_counter() - t0 < ta:
@@ -520,7 +520,10 @@ def serving_bench(lens, nsx, synth, abi, Engine, device, rates=((2000.0, 800), (
             cs = eng.sizes(p)[1]
             counts = np.zeros(cs)
             bufs.append(counts)
+            ts = time.perf_counter()
+            lag.append(1000.0 * (ts - t0 - ta))  # how late the client submits against the Poisson schedule
             tickets.append(eng.submit(p, None, counts))
+            sub.append(1000.0 * (time.perf_counter() - ts))
         lat = []
         for t in tickets:
             eng.wait(t)
@@ -529,7 +532,8 @@ def serving_bench(lens, nsx, synth, abi, Engine, device, rates=((2000.0, 800), (
         t_all = time.perf_counter() - t0
         results.append({"offered_req_per_s": rate, "requests": n, "throughput_req_per_s": n / t_all,
                         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                        "max_ms": float(np.max(lat))})
+                        "max_ms": float(np.max(lat)), "client_lag_ms_max": float(np.max(lag)),
+                        "submit_ms_p50": float(np.percentile(sub, 50)), "submit_ms_max": float(np.max(sub))})
     eng.close()
     return results
 
