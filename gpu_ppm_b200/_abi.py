@@ -96,6 +96,16 @@ class ResultInfo(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class ServeBatchTrace(ctypes.Structure):
+    _fields_ = [
+        ("t_admit", c_double), ("t_launched", c_double), ("t_finished", c_double), ("t_published", c_double),
+        ("n_requests", c_int32), ("stream_slot", c_int32), ("staging_bytes", c_int64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Fit(ctypes.Structure):
     _fields_ = [("chi2", c_double), ("loglike", c_double), ("model_total", c_double), ("n_zero_model", c_int64)]
 
@@ -144,6 +154,7 @@ SIGNATURES = {
     "ppm_wait": (c_int32, [c_void_p, c_uint64, c_int32, POINTER(ResultInfo)]),
     "ppm_ticket_latency_us": (c_int32, [c_void_p, c_uint64, POINTER(c_double)]),
     "ppm_ticket_release": (c_int32, [c_void_p, c_uint64]),
+    "ppm_serve_trace": (c_int32, [c_void_p, c_void_p, c_int32, POINTER(c_int32)]),
     "ppm_lensing_generate": (c_int32, [POINTER(LensingSpec), DP, DP, DP]),
     "ppm_response_prepare": (c_int32, [c_int32, c_int32, DP, DP, DP, DP, DP, c_int32, DP, DP]),
     "ppm_ism_inst_prepare": (c_int32, [c_char_p, c_char_p, c_char_p, c_int32, c_int32, c_int32, c_int32, c_int32,

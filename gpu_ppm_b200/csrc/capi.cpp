@@ -379,4 +379,12 @@ int ppm_ticket_release(ppm_engine* e, uint64_t ticket) {
   return guarded([&] { eng(e).release_ticket(ticket); });
 }
 
+int ppm_serve_trace(ppm_engine* e, ppm_serve_batch_trace* out, int32_t cap, int32_t* n_out) {
+  return guarded([&] {
+    if (cap < 0 || (cap > 0 && !out)) throw Error(PPM_E_INVALID, "trace buffer");
+    const int n = eng(e).serve_trace(out, cap);
+    if (n_out) *n_out = n;
+  });
+}
+
 }  // extern "C"

@@ -214,6 +214,7 @@ class Engine {
   int wait(uint64_t t, int timeout_ms, ppm_result_info* info);
   double latency_us(uint64_t t);
   void release_ticket(uint64_t t);
+  int serve_trace(ppm_serve_batch_trace* out, int cap);
   void serve_shutdown();
 
   ppm_engine_config cfg;

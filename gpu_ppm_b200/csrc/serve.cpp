@@ -8,7 +8,9 @@
 // whose device working set fits in what remains of the memory budget, builds
 // them into one batch with stream-ordered allocations and enqueues plan ->
 // integrand -> fold -> device-to-pinned copies into a staging buffer of its
-// own; batches on different streams overlap on the device.  A host callback
+// own (from a pool allocated when the server starts; a batch holds at most
+// one buffer's worth of results); batches on different streams overlap on
+// the device.  A host callback
 // after the copies marks the batch finished; the scheduler then frees its
 // stream and device memory at once and hands the staging buffer to a
 // completion thread, which copies each request's results into its
@@ -35,6 +37,7 @@ using Clock = std::chrono::steady_clock;
 namespace {
 constexpr int kMaxRequestsPerBatch = 256;
 constexpr size_t kMaxCompleting = 4;  // finished batches whose results are still being copied out
+constexpr size_t kTraceRecords = 4096;  // served batches kept for ppm_serve_trace
 
 HostBuffer take(HostBuffer& b) {
   HostBuffer r = b;
@@ -43,11 +46,15 @@ HostBuffer take(HostBuffer& b) {
   return r;
 }
 
-// staging sizes grow in powers of two (>= 1 MiB) so that a pooled buffer is rarely reallocated
-size_t staging_size(size_t bytes) {
-  size_t s = size_t(1) << 20;
-  while (s < bytes) s <<= 1;
-  return s;
+// Pinned staging: a fixed pool of kStageBytes buffers allocated when the
+// server starts, so that no pinned allocation (hundreds of ms for a few
+// hundred MB) ever runs while requests wait; admission caps a batch by the
+// bytes it stages, and only a single request larger than a buffer gets its own.
+constexpr size_t kStageBytes = size_t(32) << 20;
+constexpr size_t kStageFixed = 64 + 256;  // control words and slack around the per-request arrays
+
+size_t staged_bytes(size_t n, size_t counts, size_t flux, bool want_flux) {
+  return kStageFixed + sizeof(unsigned long long) * kStats * n + sizeof(double) * (counts + (want_flux ? flux : 0));
 }
 }  // namespace
 
@@ -84,6 +91,7 @@ struct Server {
     double* counts = nullptr;            // pinned copy of the counts pool
     double* flux = nullptr;              // pinned copy of the flux pool
     bool want_flux = false;
+    ppm_serve_batch_trace trace{};
   };
 
   Engine* eng = nullptr;
@@ -102,13 +110,30 @@ struct Server {
   uint64_t next_ticket = 1;
   bool stop = false, scheduler_done = false;
   std::thread thread, completer;
+  const Clock::time_point t_start = Clock::now();
+  std::deque<ppm_serve_batch_trace> traces;  // the last kTraceRecords batches
+
+  double since_start_us(Clock::time_point t) const {
+    return std::chrono::duration<double, std::micro>(t - t_start).count();
+  }
 
   explicit Server(Engine* e) : eng(e) {
     budget = (size_t)e->cfg.memory_budget;
     slots.resize(e->cfg.n_streams);
-    for (auto& s : slots) {
-      cudaError_t err = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
-      if (err != cudaSuccess) throw Error(PPM_E_CUDA, std::string("serving stream: ") + cudaGetErrorString(err));
+    try {
+      for (auto& s : slots) {
+        cudaError_t err = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+        if (err != cudaSuccess) throw Error(PPM_E_CUDA, std::string("serving stream: ") + cudaGetErrorString(err));
+      }
+      // enough buffers that one is always free at admission: at most n_streams - 1
+      // in flight, kMaxCompleting - 1 queued and one being copied out
+      stage_pool.resize(slots.size() + kMaxCompleting);
+      for (auto& b : stage_pool) b.reserve(kStageBytes);
+    } catch (...) {  // the destructor does not run for a constructor that throws
+      for (auto& b : stage_pool) b.release();
+      for (auto& s : slots)
+        if (s.stream) cudaStreamDestroy(s.stream);
+      throw;
     }
     // keep freed stream-ordered memory in the pool instead of returning it each time
     cudaMemPool_t pool;
@@ -145,6 +170,7 @@ struct Server {
   static void CUDART_CB on_finished(void* arg) {
     InFlight* f = (InFlight*)arg;
     Server* s = f->server;  // f may be retired and destroyed as soon as it is marked finished
+    f->trace.t_finished = s->since_start_us(Clock::now());
     f->finished.store(true);
     {
       std::lock_guard<std::mutex> lk(s->mu);
@@ -214,6 +240,10 @@ struct Server {
       auto out = copy_out(*f);
       lk.lock();
       for (auto& kv : out) done[kv.first] = kv.second;
+      f->trace.t_published = since_start_us(Clock::now());
+      f->trace.staging_bytes = (int64_t)f->stage.cap;
+      traces.push_back(f->trace);
+      if (traces.size() > kTraceRecords) traces.pop_front();
       stage_pool.push_back(take(f->stage));
       cv_done.notify_all();
       cv.notify_all();  // the scheduler may be waiting for room in the completion queue
@@ -247,13 +277,22 @@ struct Server {
         cv.wait_for(lk, std::chrono::microseconds(200));
         continue;
       }
-      // admit the oldest requests that fit the remaining budget
+      // admit the oldest requests that fit the remaining budget and one staging buffer
       std::vector<Request> take_reqs;
-      size_t bytes = 0;
+      size_t bytes = 0, counts = 0, flux = 0;
+      bool want_flux = false;
       while (!pending.empty() && (int)take_reqs.size() < kMaxRequestsPerBatch &&
              in_use + bytes + pending.front().bytes <= budget) {
-        bytes += pending.front().bytes;
-        take_reqs.push_back(pending.front());
+        const Request& r = pending.front();
+        const bool wf = want_flux || r.flux != nullptr;
+        if (!take_reqs.empty() &&
+            staged_bytes(take_reqs.size() + 1, counts + (size_t)r.n_counts, flux + (size_t)r.n_flux, wf) > kStageBytes)
+          break;
+        bytes += r.bytes;
+        counts += (size_t)r.n_counts;
+        flux += (size_t)r.n_flux;
+        want_flux = wf;
+        take_reqs.push_back(r);
         pending.pop_front();
       }
       if (take_reqs.empty()) {  // waiting for memory to free up
@@ -268,11 +307,12 @@ struct Server {
       f->slot = free_slot;
       f->bytes = bytes;
       f->reqs = std::move(take_reqs);
-      if (!stage_pool.empty()) {  // the largest pooled staging buffer
-        auto big = std::max_element(stage_pool.begin(), stage_pool.end(),
-                                    [](const HostBuffer& a, const HostBuffer& b) { return a.cap < b.cap; });
-        f->stage = take(*big);
-        stage_pool.erase(big);
+      f->trace.t_admit = since_start_us(Clock::now());
+      f->trace.n_requests = (int32_t)f->reqs.size();
+      f->trace.stream_slot = free_slot;
+      if (!stage_pool.empty()) {
+        f->stage = take(stage_pool.back());
+        stage_pool.pop_back();
       }
       lk.unlock();
       int err = PPM_OK;
@@ -281,6 +321,7 @@ struct Server {
       } catch (const Error& e) {
         err = e.code;
       }
+      f->trace.t_launched = since_start_us(Clock::now());
       lk.lock();
       if (err != PPM_OK) {
         slot.busy = false;
@@ -309,9 +350,8 @@ struct Server {
     const size_t n_counts = (size_t)B.counts_off[n], n_flux = (size_t)B.flux_off[n];
     f.want_flux = false;
     for (auto& r : f.reqs) f.want_flux |= r.flux != nullptr;
-    const size_t bytes = 64 + sizeof(unsigned long long) * kStats * n + sizeof(double) * n_counts +
-                         (f.want_flux ? sizeof(double) * n_flux : 0) + 256;
-    f.stage.reserve(staging_size(bytes));
+    const size_t bytes = staged_bytes((size_t)n, n_counts, n_flux, f.want_flux);
+    f.stage.reserve(std::max(bytes, kStageBytes));  // a no-op unless one request alone exceeds a pooled buffer
     unsigned char* h = (unsigned char*)f.stage.ptr;
     f.ctrl = (int*)h;
     f.stats = (unsigned long long*)(h + 64);
@@ -419,6 +459,15 @@ void Engine::release_ticket(uint64_t t) {
   if (!server->done.count(t)) throw Error(PPM_E_STATE, "ticket not finished");
   server->done.erase(t);
   server->known.erase(t);
+}
+
+int Engine::serve_trace(ppm_serve_batch_trace* out, int cap) {
+  if (!server) return 0;
+  std::lock_guard<std::mutex> lk(server->mu);
+  const int avail = (int)server->traces.size();
+  const int n = std::min(cap, avail);
+  for (int i = 0; i < n; ++i) out[i] = server->traces[(size_t)(avail - n + i)];
+  return n;
 }
 
 void Engine::serve_shutdown() {

@@ -179,6 +179,13 @@ class Engine:
         """Forgets a finished ticket (ppm_ticket_release)."""
         check(lib().ppm_ticket_release(self.h, ticket))
 
+    def serve_trace(self, cap=4096):
+        """The most recent served batches (ppm_serve_trace), oldest first, as dicts."""
+        buf = (_abi.ServeBatchTrace * cap)()
+        n = ctypes.c_int32()
+        check(lib().ppm_serve_trace(self.h, buf, cap, ctypes.byref(n)))
+        return [buf[i].as_dict() for i in range(n.value)]
+
 
 class Batch:
     """Wraps ppm_batch: uploads/plans once; `launch(stream)` replays a CUDA graph

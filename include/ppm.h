@@ -322,6 +322,22 @@ int ppm_ticket_latency_us(ppm_engine* e, uint64_t ticket, double* latency_us);
  * ticket has not finished. */
 int ppm_ticket_release(ppm_engine* e, uint64_t ticket);
 
+/* One served batch, times in microseconds since the server started (its first
+ * ppm_submit). */
+typedef struct ppm_serve_batch_trace {
+  double t_admit;     /* requests taken from the queue */
+  double t_launched;  /* built, uploaded and enqueued on its stream */
+  double t_finished;  /* its results reached the pinned staging buffer */
+  double t_published; /* results copied to the callers, tickets completed */
+  int32_t n_requests;
+  int32_t stream_slot;
+  int64_t staging_bytes; /* pinned staging capacity the batch used */
+} ppm_serve_batch_trace;
+
+/* The most recent served batches (at most the last 4096), oldest first:
+ * copies min(cap, available) records to out and their number to n_out. */
+int ppm_serve_trace(ppm_engine* e, ppm_serve_batch_trace* out, int32_t cap, int32_t* n_out);
+
 /* ---- tables & files ----------------------------------------------------------- */
 
 /* Generates lensing tables with the Schwarzschild ray integrals of
