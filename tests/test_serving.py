@@ -72,3 +72,21 @@ def test_invalid_request_rejected_at_submit(served):
     p.n_gl = 9
     with pytest.raises(_abi.PpmError):
         e.submit(p, np.zeros(e.sizes(p)[0]), None)
+
+
+def test_serve_trace_records_every_batch(served):
+    e, grids = served
+    before = e.serve_trace()
+    reqs = mixed_requests(grids, 24, seed=9)
+    bufs = [np.zeros(e.sizes(p)[1]) for p in reqs]
+    tickets = [e.submit(p, None, b) for p, b in zip(reqs, bufs)]
+    for t in tickets:
+        assert e.wait(t, timeout_ms=120000).status == 0
+        e.release(t)
+    new = e.serve_trace()[len(before):]
+    assert sum(b["n_requests"] for b in new) == len(reqs)
+    for b in new:
+        # the GPU may finish before the launch call returns, so finished is ordered only against admit and publish
+        assert 0 <= b["t_admit"] <= b["t_launched"] <= b["t_published"]
+        assert b["t_admit"] <= b["t_finished"] <= b["t_published"]
+        assert b["n_requests"] >= 1 and b["staging_bytes"] >= 32 << 20
