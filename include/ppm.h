@@ -166,7 +166,8 @@ typedef struct ppm_engine_config {
                                  the most device memory the engine keeps cached between synchronous calls */
   int32_t autotune;           /* 1: time candidate launch shapes at first use */
   int32_t n_streams;          /* serving: concurrent batches in flight (0 = 2: one computing while the next
-                                 is staged; more in flight measured less stable under overload) */
+                                 is staged); the server also pins n_streams + 4 staging buffers of 32 MiB
+                                 when it starts (first ppm_submit) */
 } ppm_engine_config;
 
 /* ---- engine ---------------------------------------------------------------- */
@@ -306,7 +307,8 @@ int ppm_output_sizes(ppm_engine* e, const ppm_params* p, int64_t* n_flux, int64_
 
 /* Queues a request; returns immediately with a ticket.  Requests that arrive
  * while others are on the device are admitted into the next batch as stream
- * slots and the memory budget free up.  flux / counts must stay valid until
+ * slots and the memory budget free up; a batch takes at most one 32 MiB
+ * staging buffer's worth of results.  flux / counts must stay valid until
  * the ticket completes.  Returns PPM_E_OOM if the request alone exceeds the budget. */
 int ppm_submit(ppm_engine* e, const ppm_params* p, double* flux, double* counts, uint64_t* ticket);
 /* done = 1 once the ticket finished (its status is then in info via ppm_wait). */
