@@ -1,0 +1,52 @@
+"""Host-side helpers of bench.py: its error metric is the parity tests' metric,
+the bench-workload parity check recovers a known error, and the CPU-baseline
+sample respects its time budget."""
+import types
+
+import numpy as np
+
+import bench
+import oracle
+from gpu_ppm_b200 import synth
+from tests.errors import FLOOR, max_rel
+
+
+def test_bench_metric_matches_parity_metric():
+    rng = np.random.default_rng(3)
+    ref = rng.random((300, 64)) * 10.0 ** rng.integers(-9, 1, size=(300, 64))
+    a = ref * (1 + 1e-5 * rng.standard_normal(ref.shape))
+    assert bench.REL_FLOOR == FLOOR
+    assert bench.max_rel(a, ref) == max_rel(a, ref)
+    assert bench.max_rel(np.zeros(4), np.zeros(4)) == 0.0
+
+
+def test_parity_vs_oracle_recovers_a_planted_error():
+    E = synth.energy_grid(300, 0.2, 12.0)
+    rsp = synth.response(300, 1000, E, seed=0)
+    plist = [types.SimpleNamespace(n_bins=b, exposure_s=1e6) for b in (32, 64, 128, 64, 32)]
+    rng = np.random.default_rng(1)
+    sample = np.array([3, 0, 2])
+    ref_flux = [rng.random((plist[i].n_bins, 300)) for i in sample]
+    off = np.cumsum([0] + [300 * p.n_bins for p in plist])
+    counts = np.zeros(off[-1])
+    for k, i in enumerate(sample):
+        c = oracle.fold(rsp, ref_flux[k], 1e6) * (1 + (2e-6 if k == 1 else 0.0))
+        counts[off[i]:off[i + 1]] = c.ravel()
+    out = bench.parity_vs_oracle(sample, ref_flux, plist, counts, rsp)
+    assert out["profiles"] == 3
+    assert abs(out["max_rel_err"] - 2e-6) < 1e-12
+    assert out["median_rel_err"] < 1e-12
+
+
+def test_choose_sample_respects_budget_and_spreads():
+    counts = np.arange(1, 4097) * 10
+    order = np.argsort(counts)
+    s = bench.choose_sample(order, counts, seconds=1.0, cores=4)
+    budget = 1.0 * 4 * 1e9 / 60.0
+    assert len(s) >= 1
+    assert counts[s].sum() * 64 * 2 * 300 <= budget or len(s) == 1
+    assert len(set(s.tolist())) == len(s)
+
+
+def test_cpu_model_is_reported():
+    assert isinstance(bench.cpu_model(), str) and bench.cpu_model()
