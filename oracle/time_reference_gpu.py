@@ -21,6 +21,7 @@ clamp where its CPU does, and the engine follows the CPU).  MEASUREMENT
 INFRASTRUCTURE ONLY; runs on a GPU with the reference program prebuilt.
 
     python oracle/time_reference_gpu.py [--repeats 3]
+    python oracle/time_reference_gpu.py --layout DIR [--only NAME]   # tables + scen.txt only (for a profiler)
 """
 from __future__ import annotations
 
@@ -60,10 +61,40 @@ def max_rel(a, ref, floor=1e-6):
     return float((np.abs(a - ref) / denom).max())
 
 
+def write_layout(d, lens, nsx, E, rsp, lines):
+    """The reference program's working directory: tables, NSX file, output/ and scen.txt."""
+    lens.write_dir(os.path.join(d, "tables", "lensing", "std"))
+    nsx.write_file(os.path.join(d, "ext", "model_data", "nsx_H_v200804.out"))
+    synth_mod().write_ism_inst(os.path.join(d, "tables", "ism_inst", "std"), E, rsp)
+    os.makedirs(os.path.join(d, "output"), exist_ok=True)
+    path = os.path.join(d, "scen.txt")
+    with open(path, "w") as f:
+        for ln in lines:
+            f.write(" ".join(repr(x) if isinstance(x, float) else str(x) for x in ln) + "\n")
+    return path
+
+
+def synth_mod():
+    from gpu_ppm_b200 import synth
+
+    return synth
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--repeats", type=int, default=3)
+    ap.add_argument("--layout", help="only write the reference program's working directory here and exit")
+    ap.add_argument("--only", help="scenario name for --layout")
     args = ap.parse_args()
+    if args.layout:
+        synth = synth_mod()
+        E = synth.energy_grid(300, 0.2, 12.0)
+        scen = [s for s in SCENARIOS if args.only in (None, s[0])]
+        if not scen:
+            raise SystemExit(f"unknown scenario {args.only}")
+        write_layout(args.layout, synth.lensing("std"), synth.nsx("v200804", seed=0), E,
+                     synth.response(300, 1000, E, seed=0), scen)
+        return
     prog = os.path.join(ROOT, "oracle", "_ref", "ref_devarshi_gpu")
     if not os.path.exists(prog):
         raise SystemExit(f"{prog} is missing: build it with `make -C oracle ref` where the reference sources are")
@@ -77,15 +108,8 @@ def main():
     rsp = synth.response(300, 1000, E, seed=0)
     ref_ms, ref_counts = {}, {}
     with tempfile.TemporaryDirectory() as tmp:
-        lens.write_dir(os.path.join(tmp, "tables", "lensing", "std"))
-        nsx.write_file(os.path.join(tmp, "ext", "model_data", "nsx_H_v200804.out"))
-        synth.write_ism_inst(os.path.join(tmp, "tables", "ism_inst", "std"), E, rsp)
-        os.makedirs(os.path.join(tmp, "output"))
         lines = [("Warmup",) + SCENARIOS[0][1:]] + [s for s in SCENARIOS for _ in range(args.repeats)]
-        path = os.path.join(tmp, "scen.txt")
-        with open(path, "w") as f:
-            for ln in lines:
-                f.write(" ".join(repr(x) if isinstance(x, float) else str(x) for x in ln) + "\n")
+        path = write_layout(tmp, lens, nsx, E, rsp, lines)
         p = subprocess.run([prog, path], cwd=tmp, capture_output=True, text=True, timeout=1200)
         if p.returncode != 0:
             raise SystemExit(f"reference program failed ({p.returncode}): {p.stderr[-2000:]}")
