@@ -991,6 +991,9 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
   int nt = (ne_max + ne_t - 1) / ne_t;
   nt = (nt + 31) / 32 * 32;
   nt = std::max(64, std::min(512, nt));
+  // few energies: the blackbody kernel evaluates one phase point per thread
+  // (its point-wise path, n_e * 4 <= threads), so size the block by points
+  if (!nsx_kernel && ne_max * 4 <= 256) nt = 256;
   // whole multiples of the warp count keep the one-warp-per-point build balanced
   const int nwarps = nt / 32;
   int pb = std::max(nwarps, (std::min(tune.pb, nt) / nwarps) * nwarps);

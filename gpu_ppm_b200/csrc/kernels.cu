@@ -22,6 +22,8 @@
 //      Pooled-polynomial kernel (grids with > 16 energies in one cell): one
 //      warp per point writes the cubics to shared memory, one thread per
 //      energy reads its cell's cubic.
+#include <algorithm>
+#include <climits>
 #include <cstdio>
 
 #include "kernels.cuh"
@@ -218,6 +220,87 @@ __device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtr
   if (flux == 0) return 0.0;
   z = (1 - af) * s.Z[i] + af * s.Z[i + 1];
   mu = (1 - af) * s.MU[i] + af * s.MU[i + 1];
+  return flux;
+}
+
+// Largest j in [-1, n-1] with xx[j] <= x for a non-decreasing xx (xx[-1] taken
+// as -inf), searched from `jl`, a previous answer, by doubling steps and then
+// bisection: the same index vhunt's bisection finds on such an array, in O(1)
+// steps for successive nearby x.
+__device__ __forceinline__ int hunt_from(const double* xx, int n, double x, int jl) {
+  int lo, hi;  // xx[lo] <= x < xx[hi], with xx[-1] = -inf and xx[n] = +inf
+  if (jl < 0 || x >= xx[jl]) {
+    lo = jl;
+    int step = 1;
+    hi = lo + 1;
+    while (hi < n && x >= xx[hi]) {
+      lo = hi;
+      step <<= 1;
+      hi = lo + step;
+    }
+    if (hi > n) hi = n;
+  } else {
+    hi = jl;
+    int step = 1;
+    lo = hi - 1;
+    while (lo >= 0 && x < xx[lo]) {
+      hi = lo;
+      step <<= 1;
+      lo = hi - step;
+    }
+    if (lo < -1) lo = -1;
+  }
+  while (hi - lo > 1) {
+    const int m = (lo + hi) >> 1;
+    if (x >= xx[m])
+      lo = m;
+    else
+      hi = m;
+  }
+  return lo;
+}
+
+// phase_point's arithmetic for one element at phase point i_pp, for the
+// blackbody kernel's point-wise path, with the element's phase shift
+// (phi / 2 pi) and 1 / n_bins computed once by the caller: when the tile's
+// phase_o is non-decreasing (mono), the bracket is hunted from `hint`, this
+// thread's previous one, which gives vhunt's bracket and fraction exactly.
+__device__ __forceinline__ double phase_point_at(const DevProfile& p, const SmemPtrs& s, int n_gl, double inv_bins,
+                                                 double phase_shift, int i_pp, bool mono, int& hint, int& bin,
+                                                 double& wgl, double& z) {
+  int g = 0;
+  if (n_gl > 0) {
+    bin = i_pp / n_gl;
+    g = i_pp - bin * n_gl;
+  } else {
+    bin = i_pp;
+  }
+  double ppt;
+  if (n_gl > 0) {
+    const double width = inv_bins;
+    const double lb = bin * width, ub = (bin + 1) * width;
+    ppt = 0.5 * (lb + ub + c_gl_nodes[n_gl * (n_gl - 1) / 2 + g] * (ub - lb));
+    wgl = 0.5 * 1. * c_gl_weights[n_gl * (n_gl - 1) / 2 + g];
+  } else {
+    ppt = bin * inv_bins;
+    wgl = 1.0;
+  }
+  const double xph = ppt + phase_shift + 1.;
+  double patch = xph - floor(xph);
+  if (patch < s.P[0]) patch += 1.;
+  const int n = p.n_fine + 1;
+  double af;
+  int i;
+  if (mono) {
+    hint = hunt_from(s.P, n, patch, hint);
+    i = clampi(hint, 0, n - 2);
+    af = (patch - s.P[i]) / (s.P[i + 1] - s.P[i]);
+  } else {
+    i = vhunt(s.P, n, patch, af);
+  }
+  const double flux = (1 - af) * s.F[i] + af * s.F[i + 1];
+  if (flux == 0) return 0.0;
+  z = (1 - af) * s.Z[i] + af * s.Z[i + 1];
   return flux;
 }
 
@@ -940,6 +1023,74 @@ __global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
         acc[k] = 0;
       }
     };
+    // Few energies (at most a quarter of the threads): every thread walks a
+    // run of consecutive phase points of one element and evaluates each at all
+    // energies, instead of the compacted points being walked serially by the
+    // threads that own energies.  The lanes of a warp hold consecutive elements
+    // at the same phase point, and each thread hunts its next bracket in
+    // phase_o from the last one.
+    if (n_e * 4 <= nt) {
+      bool ok = true;
+      for (int i = tid; i < p.n_fine; i += nt) ok &= s.P[i + 1] >= s.P[i];
+      const bool mono = __syncthreads_and(ok) != 0;
+      const int runs = max(1, min(n_pp, nt / n_act));  // runs of phase points per element
+      const int per_run = (n_pp + runs - 1) / runs;
+      const int n_items = n_act * runs;
+      const int lane = tid & 31;
+      const int n_gl = p.n_gl;
+      const double inv_bins = 1. / p.n_bins;
+      unsigned int n_vis = 0;
+      for (int it0 = 0; it0 < n_items; it0 += nt) {
+        const int it = it0 + tid;
+        const bool live = it < n_items;
+        const int jj = live ? it % n_act : 0;
+        const int pp0 = live ? (it / n_act) * per_run : 0;
+        const int pp1 = live ? min(n_pp, pp0 + per_run) : 0;
+        const double phase_shift = (point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs)) / kTwoPi;
+        int hint = -1;
+        for (int k = 0; k < per_run; ++k) {  // the same trip count on every lane
+          int bin = INT_MAX;  // lanes without a point: a bin after every real one
+          double c = 0, zz = 0;
+          bool vis = false;
+          if (pp0 + k < pp1) {
+            double wgl, z = 0;
+            const double flux = phase_point_at(p, s, n_gl, inv_bins, phase_shift, pp0 + k, mono, hint, bin, wgl, z);
+            if (flux != 0.0) {
+              vis = true;
+              c = flux * wgl;
+              zz = z;
+            }
+          }
+          n_vis += vis ? 1u : 0u;
+          // bins never decrease along the lanes (consecutive elements of one run
+          // share the phase point; later runs have later points; lanes without a
+          // point come last), so the lanes of one bin are one run of lanes, summed
+          // by a segmented shuffle reduction into the run's first lane
+          const int prev_bin = __shfl_up_sync(0xffffffffu, bin, 1);
+          const bool head = (lane == 0 || prev_bin != bin) && bin != INT_MAX;
+          const Real cb = (Real)c, zb = (Real)zz;
+          for (int e = 0; e < n_e; ++e) {
+            Real v = 0;
+            if (vis) {
+              const Real Ee = (Real)G.E[e] * zb;
+              v = cb * (Ee * Ee * Ee / expm1(Ee / kT));  // Ibb without its constant (in out_scale)
+            }
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+              const Real o = __shfl_down_sync(0xffffffffu, v, off);
+              const int ob = __shfl_down_sync(0xffffffffu, bin, off);
+              if (lane + off < 32 && ob == bin) v += o;
+            }
+            if (head && v != (Real)0)
+              atomicAdd(flux_base + (size_t)bin * n_e + e, (double)v * out_scale * G.invE[e]);
+          }
+        }
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) n_vis += __shfl_down_sync(0xffffffffu, n_vis, off);
+      if (lane == 0 && n_vis) atomicAdd(&p.stats[3], (unsigned long long)n_vis);
+      continue;
+    }
     for (int q0 = 0; q0 < n_pts; q0 += nt) {
       bool vis = false;
       double c = 0, zz = 0;
@@ -1053,15 +1204,19 @@ __device__ __forceinline__ void push_tile(const WorkQueue& q, const Tile& t) {
     atomicOr(q.overflow, 1);
 }
 
-__global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const DevLens L, const WorkQueue q, int chunk) {
-  const int pi = blockIdx.x / kMaxSpots, si = blockIdx.x % kMaxSpots;
+// One CTA per (profile, spot, ring block): a spot's rings are shared by
+// ring_blocks CTAs, so that a small batch plans on many SMs at once.
+__global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const DevLens L, const WorkQueue q, int chunk,
+                            int ring_blocks) {
+  const int ps = blockIdx.x / ring_blocks, rb = blockIdx.x - ps * ring_blocks;
+  const int pi = ps / kMaxSpots, si = ps % kMaxSpots;
   if (pi >= n_profiles) return;
   const DevProfile& p = profiles[pi];
   if (si >= p.n_spots) return;
   const DevSpot& sp = p.spot[si];
   const bool nsx = p.atmosphere == 0;
   if (sp.kind == 1) {
-    if (sp.i_lo > sp.i_hi) return;  // outside the batch's ring window
+    if (sp.i_lo > sp.i_hi || rb != 0) return;  // outside the batch's ring window, or another block's
     if (threadIdx.x == 0) {
       RingGeom g;
       ring_geometry(p, L, sp.cos_theta_pt, sp.dOmega_pt, false, g);
@@ -1076,7 +1231,7 @@ __global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const De
     return;
   }
   const int N = p.n_side;
-  for (int i = sp.i_lo + threadIdx.x; i <= sp.i_hi; i += blockDim.x) {
+  for (int i = sp.i_lo + rb * (int)blockDim.x + (int)threadIdx.x; i <= sp.i_hi; i += ring_blocks * (int)blockDim.x) {
     const double z = p.ring[3 * i], c2 = p.ring[3 * i + 1], s2 = p.ring[3 * i + 2];
     const int jmax = healpix_jmax(N, i);
     int r[2][2];
@@ -1284,7 +1439,9 @@ int max_active_ctas(const IntegrandShape& s) {
 cudaError_t launch_plan(const DevProfile* profiles, int n_profiles, const DevLens& lens, const WorkQueue& q, int chunk,
                         cudaStream_t st) {
   if (n_profiles <= 0) return cudaSuccess;
-  plan_kernel<<<n_profiles * kMaxSpots, 128, 0, st>>>(profiles, n_profiles, lens, q, chunk);
+  // a few profiles: up to 32 CTAs share each spot's rings (4N - 1 of them at most)
+  const int ring_blocks = std::max(1, std::min(32, 64 / n_profiles));
+  plan_kernel<<<n_profiles * kMaxSpots * ring_blocks, 128, 0, st>>>(profiles, n_profiles, lens, q, chunk, ring_blocks);
   return cudaGetLastError();
 }
 

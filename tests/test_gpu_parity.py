@@ -101,6 +101,38 @@ def test_config1_blackbody_fp64():
     e.close()
 
 
+def test_blackbody_pointwise_and_energy_paths(golden, eng_v200804, ora_v200804):
+    """The blackbody kernel evaluates one phase point per thread when a grid has
+    few energies (n_e * 4 <= threads) and walks compacted points per energy
+    otherwise; both, in FP32 and FP64, against the oracle, alone and mixed in
+    one batch (the path is chosen per tile)."""
+    meta, _ = golden
+    few = []
+    for s in meta["os1"][:4]:
+        for prec, tol in ((_abi.PREC_FP32, TOL32), (_abi.PREC_FP64, TOL64)):
+            p = gc.os1_params(s, eng_v200804.g1)
+            p.precision = prec
+            flux, _, _ = eng_v200804.profile(p)
+            ref, _ = ora_v200804.profile(p, np.array([1.0]))
+            assert max_rel(flux, ref) < tol, (s[0], prec)
+            few.append((p, ref))
+    lens = synth.lensing("std")
+    E = synth.energy_grid(300, 0.2, 10.0)
+    e = Engine()
+    e.load_lensing(lens)
+    g300, g1 = e.add_energy_grid(E), e.add_energy_grid(np.array([1.0]))
+    many = synth.config1_params(g300)
+    flux, _, _ = e.profile(many)
+    ref_many, _ = oracle.Oracle(lens).profile(many, E)
+    assert max_rel(flux, ref_many) < TOL64
+    p1 = few[1][0]
+    p1.energy_grid = g1
+    fb, _, _ = e.profile_batch([many, p1], want_flux=True, want_counts=False)
+    assert max_rel(fb[0], ref_many) < TOL64
+    assert max_rel(fb[1], few[1][1]) < TOL64
+    e.close()
+
+
 @pytest.fixture(scope="module")
 def eng_v171019():
     lens, nsx = synth.lensing("std"), synth.nsx("v171019", seed=0)
