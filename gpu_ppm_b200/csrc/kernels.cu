@@ -24,6 +24,7 @@
 //      energy reads its cell's cubic.
 #include <algorithm>
 #include <climits>
+#include <cstdint>
 #include <cstdio>
 
 #include "kernels.cuh"
@@ -261,13 +262,16 @@ __device__ __forceinline__ int hunt_from(const double* xx, int n, double x, int 
 }
 
 // phase_point's arithmetic for one element at phase point i_pp, for the
-// blackbody kernel's point-wise path, with the element's phase shift
-// (phi / 2 pi) and 1 / n_bins computed once by the caller: when the tile's
-// phase_o is non-decreasing (mono), the bracket is hunted from `hint`, this
-// thread's previous one, which gives vhunt's bracket and fraction exactly.
-__device__ __forceinline__ double phase_point_at(const DevProfile& p, const SmemPtrs& s, int n_gl, double inv_bins,
-                                                 double phase_shift, int i_pp, bool mono, int& hint, int& bin,
-                                                 double& wgl, double& z) {
+// blackbody kernel's point-wise path, with the per-tile and per-element terms
+// (n = n_fine + 1, phase_o[0], 1 / n_bins, the element's phase shift
+// phi / 2 pi) computed once by the caller.  When the tile's phase_o is
+// non-decreasing (mono), the bracket is hunted from `hint`, this thread's
+// previous one, which gives vhunt's bracket exactly, and the fraction uses
+// the tile's reciprocal interval widths inv_dp when given (within an ulp of
+// vhunt's division).
+__device__ __forceinline__ double phase_point_at(const SmemPtrs& s, int n, double P0, const double* inv_dp, int n_gl,
+                                                 double inv_bins, double phase_shift, int i_pp, bool mono, int& hint,
+                                                 int& bin, double& wgl, double& z) {
   int g = 0;
   if (n_gl > 0) {
     bin = i_pp / n_gl;
@@ -287,14 +291,13 @@ __device__ __forceinline__ double phase_point_at(const DevProfile& p, const Smem
   }
   const double xph = ppt + phase_shift + 1.;
   double patch = xph - floor(xph);
-  if (patch < s.P[0]) patch += 1.;
-  const int n = p.n_fine + 1;
+  if (patch < P0) patch += 1.;
   double af;
   int i;
   if (mono) {
     hint = hunt_from(s.P, n, patch, hint);
     i = clampi(hint, 0, n - 2);
-    af = (patch - s.P[i]) / (s.P[i + 1] - s.P[i]);
+    af = inv_dp ? (patch - s.P[i]) * inv_dp[i] : (patch - s.P[i]) / (s.P[i + 1] - s.P[i]);
   } else {
     i = vhunt(s.P, n, patch, af);
   }
@@ -973,7 +976,7 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
 
 // ---------------------------------------------------------------------------
 template <typename Real, int NE_T>
-__global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
+__global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
   const IntegrandShape& S = a.shape;
   const SmemPtrs s = carve(sm, S);
@@ -1030,15 +1033,36 @@ __global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
     // at the same phase point, and each thread hunts its next bracket in
     // phase_o from the last one.
     if (n_e * 4 <= nt) {
+      const int n_fine = p.n_fine;
       bool ok = true;
-      for (int i = tid; i < p.n_fine; i += nt) ok &= s.P[i + 1] >= s.P[i];
+      for (int i = tid; i < n_fine; i += nt) ok &= s.P[i + 1] >= s.P[i];
       const bool mono = __syncthreads_and(ok) != 0;
+      // per tile, in the lensing-row space the sweep no longer needs: reciprocal
+      // phase_o interval widths, the energies and 1/E (when they fit)
+      double* inv_dp = (double*)s.rows;
+      Real* E_s = (Real*)(inv_dp + n_fine);
+      double* invE_s = (double*)(((uintptr_t)(E_s + n_e) + 7) & ~(uintptr_t)7);
+      const bool staged = (long)((unsigned char*)(invE_s + n_e) - (unsigned char*)s.rows) <= (long)(S.total - S.off_rows);
+      if (staged) {
+        if (mono)
+          for (int i = tid; i < n_fine; i += nt) inv_dp[i] = 1.0 / (s.P[i + 1] - s.P[i]);
+        for (int e = tid; e < n_e; e += nt) {
+          E_s[e] = (Real)G.E[e];
+          invE_s[e] = G.invE[e];
+        }
+      }
+      __syncthreads();
+      const double* inv_dp_use = (staged && mono) ? inv_dp : nullptr;
+      const int n_fp = n_fine + 1;
+      const double P0 = s.P[0];
+      const Real inv_kT = (Real)1 / kT;
       const int runs = max(1, min(n_pp, nt / n_act));  // runs of phase points per element
       const int per_run = (n_pp + runs - 1) / runs;
       const int n_items = n_act * runs;
       const int lane = tid & 31;
       const int n_gl = p.n_gl;
       const double inv_bins = 1. / p.n_bins;
+      const double scale = out_scale;
       unsigned int n_vis = 0;
       for (int it0 = 0; it0 < n_items; it0 += nt) {
         const int it = it0 + tid;
@@ -1054,7 +1078,8 @@ __global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
           bool vis = false;
           if (pp0 + k < pp1) {
             double wgl, z = 0;
-            const double flux = phase_point_at(p, s, n_gl, inv_bins, phase_shift, pp0 + k, mono, hint, bin, wgl, z);
+            const double flux =
+                phase_point_at(s, n_fp, P0, inv_dp_use, n_gl, inv_bins, phase_shift, pp0 + k, mono, hint, bin, wgl, z);
             if (flux != 0.0) {
               vis = true;
               c = flux * wgl;
@@ -1072,8 +1097,8 @@ __global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
           for (int e = 0; e < n_e; ++e) {
             Real v = 0;
             if (vis) {
-              const Real Ee = (Real)G.E[e] * zb;
-              v = cb * (Ee * Ee * Ee / expm1(Ee / kT));  // Ibb without its constant (in out_scale)
+              const Real Ee = (staged ? E_s[e] : (Real)G.E[e]) * zb;
+              v = cb * (Ee * Ee * Ee / expm1(Ee * inv_kT));  // Ibb without its constant (in out_scale)
             }
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
@@ -1082,7 +1107,7 @@ __global__ void __launch_bounds__(512) integrand_bb_kernel(const KernelArgs a) {
               if (lane + off < 32 && ob == bin) v += o;
             }
             if (head && v != (Real)0)
-              atomicAdd(flux_base + (size_t)bin * n_e + e, (double)v * out_scale * G.invE[e]);
+              atomicAdd(flux_base + (size_t)bin * n_e + e, (double)v * scale * (staged ? invE_s[e] : G.invE[e]));
           }
         }
       }
