@@ -101,7 +101,7 @@ struct WorkQueue {
 };
 
 // ---- helpers ----------------------------------------------------------------
-__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+__host__ __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 // UniformHunt::operator() (cpu/hunt.hpp:98-121): clamps x to the grid.
 __device__ __forceinline__ int uhunt(double& x, double lo, double hi, int n, double& a) {
@@ -123,7 +123,7 @@ __device__ __forceinline__ int uhunt(double& x, double lo, double hi, int n, dou
 
 // VecHunt::operator() on a strictly monotone table (cpu/hunt.hpp:14-66):
 // bracket with index clamped to [0, n-2] and extrapolated fraction.
-__device__ __forceinline__ int vhunt(const double* xx, int n, double x, double& a) {
+__host__ __device__ __forceinline__ int vhunt(const double* xx, int n, double x, double& a) {
   bool ascnd = xx[n - 1] >= xx[0];
   int jl = -1, ju = n;
   while (ju - jl > 1) {
@@ -136,6 +136,43 @@ __device__ __forceinline__ int vhunt(const double* xx, int n, double x, double& 
   int i = clampi(jl, 0, n - 2);
   a = (x - xx[i]) / (xx[i + 1] - xx[i]);
   return i;
+}
+
+// Largest j in [-1, n-1] with xx[j] <= x for a non-decreasing xx (xx[-1] taken
+// as -inf), searched from `jl`, a previous answer, by doubling steps and then
+// bisection: the same index vhunt's bisection finds on such an array, in O(1)
+// steps for successive nearby x.
+__host__ __device__ __forceinline__ int hunt_from(const double* xx, int n, double x, int jl) {
+  int lo, hi;  // xx[lo] <= x < xx[hi], with xx[-1] = -inf and xx[n] = +inf
+  if (jl < 0 || x >= xx[jl]) {
+    lo = jl;
+    int step = 1;
+    hi = lo + 1;
+    while (hi < n && x >= xx[hi]) {
+      lo = hi;
+      step <<= 1;
+      hi = lo + step;
+    }
+    if (hi > n) hi = n;
+  } else {
+    hi = jl;
+    int step = 1;
+    lo = hi - 1;
+    while (lo >= 0 && x < xx[lo]) {
+      hi = lo;
+      step <<= 1;
+      lo = hi - step;
+    }
+    if (lo < -1) lo = -1;
+  }
+  while (hi - lo > 1) {
+    const int m = (lo + hi) >> 1;
+    if (x >= xx[m])
+      lo = m;
+    else
+      hi = m;
+  }
+  return lo;
 }
 
 // cpu/nsx.hpp:159-168

@@ -224,43 +224,6 @@ __device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtr
   return flux;
 }
 
-// Largest j in [-1, n-1] with xx[j] <= x for a non-decreasing xx (xx[-1] taken
-// as -inf), searched from `jl`, a previous answer, by doubling steps and then
-// bisection: the same index vhunt's bisection finds on such an array, in O(1)
-// steps for successive nearby x.
-__device__ __forceinline__ int hunt_from(const double* xx, int n, double x, int jl) {
-  int lo, hi;  // xx[lo] <= x < xx[hi], with xx[-1] = -inf and xx[n] = +inf
-  if (jl < 0 || x >= xx[jl]) {
-    lo = jl;
-    int step = 1;
-    hi = lo + 1;
-    while (hi < n && x >= xx[hi]) {
-      lo = hi;
-      step <<= 1;
-      hi = lo + step;
-    }
-    if (hi > n) hi = n;
-  } else {
-    hi = jl;
-    int step = 1;
-    lo = hi - 1;
-    while (lo >= 0 && x < xx[lo]) {
-      hi = lo;
-      step <<= 1;
-      lo = hi - step;
-    }
-    if (lo < -1) lo = -1;
-  }
-  while (hi - lo > 1) {
-    const int m = (lo + hi) >> 1;
-    if (x >= xx[m])
-      lo = m;
-    else
-      hi = m;
-  }
-  return lo;
-}
-
 // phase_point's arithmetic for one element at phase point i_pp, for the
 // blackbody kernel's point-wise path, with the per-tile and per-element terms
 // (n = n_fine + 1, phase_o[0], 1 / n_bins, the element's phase shift
