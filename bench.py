@@ -53,7 +53,40 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--probe-ranks", action="store_true",
+                    help="check the rank launch only: every rank joins a gloo group and prints its rank and the "
+                         "group size (no GPU work)")
     return ap.parse_args()
+
+
+def launch_ranks(n, argv):
+    """Runs this script as n ranks on this node (torch.distributed.run, rendezvous on 127.0.0.1) and returns
+    the launcher's exit status.  Used when --gpus N > 1 is given outside a launcher (no WORLD_SIZE)."""
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *argv]
+    return subprocess.call(cmd)
+
+
+def probe_ranks():
+    """Each rank reports its rank, the launcher's WORLD_SIZE and the size of the process group it joined."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    seen = torch.tensor([1.0])
+    dist.all_reduce(seen)
+    line = json.dumps({"probe": "ranks", "rank": dist.get_rank(), "world_size": int(os.environ.get("WORLD_SIZE", "1")),
+                       "ranks_seen": int(seen.item()), "group_size": dist.get_world_size()})
+    os.write(1, (line + "\n").encode())  # one write per line: the ranks share the launcher's stdout
+    dist.barrier()
+    dist.destroy_process_group()
 
 
 def workload(n, seed, synth, abi, g, r):
@@ -250,6 +283,11 @@ def choose_sample(order, counts, seconds, cores, offset=0, ns_per_eval=60.0):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl != "reference":
+        sys.exit(launch_ranks(args.gpus, sys.argv[1:]))
+    if args.probe_ranks:
+        probe_ranks()
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -269,6 +307,9 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        ranks_seen = dist.get_world_size()
+    else:
+        ranks_seen = 1
 
     lens, nsx = synth.lensing("wide"), synth.nsx("v171019", seed=0)
     E = synth.energy_grid(300, 0.2, 12.0)
@@ -410,7 +451,8 @@ def main():
     batch.close()
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "profiles/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": value, "unit": "profiles/s", "n_gpus": world, "ranks_seen": ranks_seen,
+            "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded tables of the reference's shapes)",
             "config": {
@@ -435,7 +477,7 @@ def main():
                 "note": "the convention counts 80 FLOP per evaluation; the kernel contracts mu once per slice row "
                         "and builds each cubic once per cell per phase point, so it executes fewer operations per "
                         "evaluation and frac can exceed 1; its hardware bound is instruction issue with the FMA and ALU pipes (74 % of issue "
-                        "slots, profiles/integrand_nsx_cell_96profiles.md)",
+                        "slots in the ncu capture of a 96-profile launch)",
             },
             "phases_ms": {"clear_plan": float(ph[0]), "integrand": float(ph[1]), "fold": float(ph[2])},
             "plain": {"value": plain_value, "unit": "profiles/s", "profiles": n_plain,

@@ -639,6 +639,7 @@ void Engine::fill_profile(const ppm_params& p, DevProfile& d, long long flux_off
 // records the launch shapes; the batch owns all of its device memory.
 void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t copy_stream, int ring_begin,
                          int ring_end, int chunk_override) {
+  NvtxRange range("batch build");
   if (n < 1) throw Error(PPM_E_INVALID, "empty batch");
   if (ring_begin > ring_end) throw Error(PPM_E_INVALID, "ring window with begin > end");
   if (!B.mem.stream) B.mem.cache = &block_cache;
@@ -786,13 +787,20 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
 void Engine::batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events) {
   const int n = B.n;
   if (events) PPM_CUDA(cudaEventRecord(events[0], st));
-  PPM_CUDA(cudaMemsetAsync(B.d_flux, 0, sizeof(double) * (size_t)B.flux_off[n], st));
-  PPM_CUDA(cudaMemsetAsync(B.d_stats, 0, sizeof(unsigned long long) * kStats * (size_t)n, st));
-  PPM_CUDA(cudaMemsetAsync(B.d_ctrl, 0, sizeof(int) * 16, st));
-  for (const auto& G : B.groups) PPM_CUDA(launch_plan(B.d_prof + G.g0, G.g1 - G.g0, lens, G.args.queue, B.chunk, st));
+  {
+    NvtxRange range("clear + plan");
+    PPM_CUDA(cudaMemsetAsync(B.d_flux, 0, sizeof(double) * (size_t)B.flux_off[n], st));
+    PPM_CUDA(cudaMemsetAsync(B.d_stats, 0, sizeof(unsigned long long) * kStats * (size_t)n, st));
+    PPM_CUDA(cudaMemsetAsync(B.d_ctrl, 0, sizeof(int) * 16, st));
+    for (const auto& G : B.groups) PPM_CUDA(launch_plan(B.d_prof + G.g0, G.g1 - G.g0, lens, G.args.queue, B.chunk, st));
+  }
   if (events) PPM_CUDA(cudaEventRecord(events[1], st));
-  for (const auto& G : B.groups) PPM_CUDA(launch_integrand(G.args, G.grid, st));
+  {
+    NvtxRange range("integrand");
+    for (const auto& G : B.groups) PPM_CUDA(launch_integrand(G.args, G.grid, st));
+  }
   if (events) PPM_CUDA(cudaEventRecord(events[2], st));
+  NvtxRange fold_range("fold");
   for (const auto& f : B.folds) {
     const Resp& r = resps[f.resp];
     const FoldJob* jobs = B.d_jobs + f.job0;
@@ -849,6 +857,7 @@ void Engine::batch_launch(BatchImpl& B, cudaStream_t st) {
 }
 
 void Engine::batch_collect(BatchImpl& B, double* flux, double* counts, ppm_result_info* info, cudaStream_t st) {
+  NvtxRange range("collect");
   PPM_CUDA(cudaSetDevice(cfg.device));
   if (!st) st = B.last_stream ? B.last_stream : stream;
   const int n = B.n;
@@ -887,6 +896,7 @@ void Engine::batch_collect(BatchImpl& B, double* flux, double* counts, ppm_resul
 }
 
 void Engine::profile(const ppm_params& p, double* flux, double* counts, ppm_result_info* info) {
+  NvtxRange range("ppm_profile");
   std::lock_guard<std::mutex> lk(mu);
   if (counts && p.response < 0) throw Error(PPM_E_INVALID, "counts requested without a response");
   BatchImpl B;
@@ -931,6 +941,7 @@ void Engine::profile_rings(const ppm_params& p, int ring_begin, int ring_end, do
 }
 
 void Engine::profile_batch(int n, const ppm_params* ps, double* flux, double* counts, ppm_result_info* info) {
+  NvtxRange range("ppm_profile_batch");
   std::lock_guard<std::mutex> lk(mu);
   BatchImpl B;
   batch_build(B, n, ps);
@@ -1010,6 +1021,7 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
 
 // Coordinate descent over the integrand's launch shape on a sample batch.
 std::string Engine::autotune(int n, const ppm_params* sample) {
+  NvtxRange range("autotune");
   std::lock_guard<std::mutex> lk(mu);
   PPM_CUDA(cudaSetDevice(cfg.device));
   const Tuning start = tune;

@@ -16,10 +16,34 @@
 #include <unordered_map>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/ppm.h"
 #include "kernels.cuh"
 
 namespace ppm {
+
+// NVTX range in the "ppm_b200" domain for the lifetime of the object: names the
+// host phases (build, plan, integrand, fold, collect, served batches) in a
+// profiler timeline.  Without a profiler attached a push/pop is one call into
+// an empty function.
+inline nvtxDomainHandle_t nvtx_domain() {
+  static nvtxDomainHandle_t d = nvtxDomainCreateA("ppm_b200");
+  return d;
+}
+struct NvtxRange {
+  explicit NvtxRange(const char* name) {
+    nvtxEventAttributes_t a{};
+    a.version = NVTX_VERSION;
+    a.size = NVTX_EVENT_ATTRIB_STRUCT_SIZE;
+    a.messageType = NVTX_MESSAGE_TYPE_ASCII;
+    a.message.ascii = name;
+    nvtxDomainRangePushEx(nvtx_domain(), &a);
+  }
+  ~NvtxRange() { nvtxDomainRangePop(nvtx_domain()); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Host rows of the per-N_side ring table and the per-n_fine phase table.
 void compute_ring_rows(int N, std::vector<double>& h);

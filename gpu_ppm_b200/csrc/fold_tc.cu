@@ -305,12 +305,10 @@ void Engine::fold_tc_prepare(Resp& r) {
 
 cudaError_t Engine::fold_tc_launch(const Resp& r, const FoldJob* jobs, int n_jobs, int n_bins, const double* flux,
                                    double* counts, cudaStream_t st) {
-  static bool configured = false;
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(fold_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  cudaError_t e = once_per_device(1, [] {
+    return cudaFuncSetAttribute(fold_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  });
+  if (e != cudaSuccess) return e;
   TcArgs a{};
   a.a_hi = (const uint16_t*)r.d_a_hi;
   a.a_lo = (const uint16_t*)r.d_a_lo;

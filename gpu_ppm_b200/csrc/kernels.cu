@@ -26,6 +26,7 @@
 #include <climits>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 
 #include "kernels.cuh"
 
@@ -1386,10 +1387,27 @@ void* kernel_for(const IntegrandShape& s, int precision) {
 }
 }  // namespace
 
-cudaError_t configure_integrand_smem(const IntegrandShape& s) {
-  // all variants get the largest dynamic shared memory allowance once
-  static bool done = false;
-  if (done) return cudaSuccess;
+namespace {
+constexpr int kOnceSlots = 4, kOnceDevices = 64;
+std::mutex g_once_mu;
+bool g_once_done[kOnceSlots][kOnceDevices];
+}  // namespace
+
+cudaError_t once_per_device(int slot, cudaError_t (*set_up)()) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (slot < 0 || slot >= kOnceSlots || dev < 0 || dev >= kOnceDevices) return set_up();
+  std::lock_guard<std::mutex> lk(g_once_mu);
+  if (g_once_done[slot][dev]) return cudaSuccess;
+  e = set_up();
+  if (e == cudaSuccess) g_once_done[slot][dev] = true;
+  return e;
+}
+
+namespace {
+// every integrand variant gets the largest dynamic shared-memory allowance of the current device
+cudaError_t set_integrand_smem() {
   void* fns[] = {(void*)integrand_nsx_cell_kernel<4, 1, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 1, 384, 2>,
                  (void*)integrand_nsx_cell_kernel<4, 2, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 2, 384, 2>,
                  (void*)integrand_nsx_cell_kernel<4, 3, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 3, 384, 2>,
@@ -1413,9 +1431,11 @@ cudaError_t configure_integrand_smem(const IntegrandShape& s) {
     e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)at.sharedSizeBytes);
     if (e != cudaSuccess) return e;
   }
-  done = true;
   return cudaSuccess;
 }
+}  // namespace
+
+cudaError_t configure_integrand_smem(const IntegrandShape&) { return once_per_device(0, set_integrand_smem); }
 
 int max_active_ctas(const IntegrandShape& s) {
   int n = 0;

@@ -54,6 +54,11 @@ struct FoldJob {
 cudaError_t launch_fold_simt(const FoldJob* jobs, int n_jobs, const double* rsp, int n_ch, int n_e, int n_bins,
                              const double* flux, double* counts, bool fp64, cudaStream_t st);
 int max_active_ctas(const IntegrandShape& s);
+// Raises the dynamic shared-memory limit of every integrand variant on the
+// current device; done once per device, safe to call from several threads.
 cudaError_t configure_integrand_smem(const IntegrandShape& s);
+// Runs `set_up` once per device ordinal (the current device), under a lock;
+// a failed set-up is retried by the next call.
+cudaError_t once_per_device(int slot, cudaError_t (*set_up)());
 
 }  // namespace ppm

@@ -237,7 +237,11 @@ struct Server {
       std::unique_ptr<InFlight> f = std::move(completing.front());
       completing.pop_front();
       lk.unlock();
-      auto out = copy_out(*f);
+      std::vector<std::pair<uint64_t, Done>> out;
+      {
+        NvtxRange range("serve batch: publish");
+        out = copy_out(*f);
+      }
       lk.lock();
       for (auto& kv : out) done[kv.first] = kv.second;
       f->trace.t_published = since_start_us(Clock::now());
@@ -335,6 +339,7 @@ struct Server {
   }
 
   void launch(InFlight& f, Slot& slot) {
+    NvtxRange range("serve batch: build + enqueue");
     const int n = (int)f.reqs.size();
     std::vector<ppm_params> ps(n);
     for (int i = 0; i < n; ++i) ps[i] = f.reqs[i].p;

@@ -23,7 +23,7 @@ _LIBS = {}
 
 def build(ref=False):
     """Builds the oracle (and, when the reference sources exist, the reference harness)."""
-    targets = ["oracle"] + (["ref"] if ref else [])
+    targets = ["oracle"] + (["ref"] if ref else [])  # "ref" needs PPM_REFERENCE_DIR
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 

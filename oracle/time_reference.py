@@ -10,7 +10,7 @@ therefore times the restatement, and this ratio tells how far that stands for
 the reference's own code.  TEST INFRASTRUCTURE ONLY; needs the reference
 sources (the Makefile's REF) and runs on the host cores.
 
-    python oracle/time_reference.py [--ref /root/reference] [--n-side 96]
+    python oracle/time_reference.py --ref <reference source tree>  (or set PPM_REFERENCE_DIR) [--n-side 96]
 """
 from __future__ import annotations
 
@@ -34,7 +34,8 @@ PI = math.pi
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PPM_REFERENCE_DIR"), required="PPM_REFERENCE_DIR" not in os.environ,
+                    help="reference source tree (default: $PPM_REFERENCE_DIR)")
     ap.add_argument("--n-side", type=int, default=96)
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.ref}"], check=True)

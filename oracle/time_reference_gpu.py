@@ -147,7 +147,7 @@ def engine_times(eng, prm, repeats, want_counts):
 def os1(args):
     prog = os.path.join(ROOT, "oracle", "_ref", "ref_os1_gpu")
     if not os.path.exists(prog):
-        raise SystemExit(f"{prog} is missing: build it with `make -C oracle ref` where the reference sources are")
+        raise SystemExit(f"{prog} is missing: build it with `make -C oracle ref REF=<reference source tree>` where the reference sources are")
     from gpu_ppm_b200 import _abi, synth
     from gpu_ppm_b200.engine import Engine
 

@@ -3,8 +3,8 @@ reference's OWN CPU programs (cpu/devarshi24st_cpu.cpp, cpu/os1_cpu.cpp,
 cpu/t_interp.cpp from fizban007/gpu_ppm, compiled unchanged by oracle/Makefile
 and driven by oracle/ref_harness.cpp) on seeded synthetic tables.
 
-Run in a container that has the reference sources (default /root/reference):
-    python tests/golden/make_golden.py [--ref /root/reference]
+Run in a container that has the reference sources:
+    python tests/golden/make_golden.py --ref <reference source tree>  (or set PPM_REFERENCE_DIR)
 
 Inputs (all regenerated bit-identically by the tests from the same seeds):
   * tables/lensing/std      synth.lensing("std")               (c_lensing.py grid)
@@ -74,7 +74,8 @@ def ism_inst():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PPM_REFERENCE_DIR"), required="PPM_REFERENCE_DIR" not in os.environ,
+                    help="reference source tree (default: $PPM_REFERENCE_DIR)")
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={args.ref}"], check=True)
     bin_dir = os.path.join(ROOT, "oracle", "_ref")

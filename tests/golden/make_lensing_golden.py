@@ -3,7 +3,7 @@
 rows u[0,85,170,255] x every 16th cos psi / cos alpha column of the three
 tables in tests/golden/lensing_std_subset.npz.
 
-    python tests/golden/make_lensing_golden.py [--ref /root/reference] [--from DIR]
+    python tests/golden/make_lensing_golden.py --ref <reference source tree>  (or set PPM_REFERENCE_DIR) [--from DIR]
 """
 import argparse
 import os
@@ -20,7 +20,8 @@ COLS = slice(0, 512, 16)
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PPM_REFERENCE_DIR"), required="PPM_REFERENCE_DIR" not in os.environ,
+                    help="reference source tree (default: $PPM_REFERENCE_DIR)")
     ap.add_argument("--from", dest="src", default=None, help="existing tables/lensing/std folder")
     a = ap.parse_args()
     with tempfile.TemporaryDirectory() as tmp:
