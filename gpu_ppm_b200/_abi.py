@@ -142,6 +142,7 @@ SIGNATURES = {
     "ppm_batch_launch_timed": (c_int32, [c_void_p, c_void_p, c_void_p, POINTER(ctypes.c_float)]),
     "ppm_batch_kernel_count": (c_int32, [c_void_p, c_void_p, POINTER(c_int32)]),
     "ppm_profile_noalloc": (c_int32, [c_void_p, POINTER(Params), c_void_p, c_void_p, c_void_p]),
+    "ppm_profile_noalloc_result": (c_int32, [c_void_p, c_void_p, POINTER(ResultInfo)]),
     "ppm_batch_create_rings": (c_int32, [c_void_p, c_int32, POINTER(Params), c_int32, c_int32, POINTER(c_void_p)]),
     "ppm_profile_rings": (c_int32, [c_void_p, POINTER(Params), c_int32, c_int32, DP, DP, POINTER(ResultInfo)]),
     "ppm_engine_add_observed": (c_int32, [c_void_p, c_int32, c_int32, DP, POINTER(c_int32)]),
@@ -149,6 +150,8 @@ SIGNATURES = {
     "ppm_profile_fit": (c_int32, [c_void_p, POINTER(Params), c_int32, POINTER(Fit), POINTER(ResultInfo)]),
     "ppm_engine_autotune": (c_int32, [c_void_p, c_int32, POINTER(Params), c_char_p, c_int32]),
     "ppm_output_sizes": (c_int32, [c_void_p, POINTER(Params), POINTER(c_int64), POINTER(c_int64)]),
+    "ppm_fold": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_int32, DP, DP, DP]),
+    "ppm_fold_device": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_int32, DP, c_void_p, c_void_p, c_void_p]),
     "ppm_submit": (c_int32, [c_void_p, POINTER(Params), DP, DP, POINTER(c_uint64)]),
     "ppm_poll": (c_int32, [c_void_p, c_uint64, POINTER(c_int32)]),
     "ppm_wait": (c_int32, [c_void_p, c_uint64, c_int32, POINTER(ResultInfo)]),

@@ -328,6 +328,16 @@ int ppm_profile_noalloc(ppm_engine* e, const ppm_params* p, double* flux_device,
   });
 }
 
+int ppm_profile_noalloc_result(ppm_engine* e, void* stream, ppm_result_info* info) {
+  int code = PPM_OK;
+  const int rc = guarded([&] { code = eng(e).profile_noalloc_result((cudaStream_t)stream, info); });
+  if (rc != PPM_OK) return rc;
+  if (code == PPM_E_RANGE) return ppm::set_error(code, "ppm_profile_noalloc: the work queue overflowed");
+  if (code == PPM_E_TIMEOUT)
+    return ppm::set_error(code, "ppm_profile_noalloc: a bounded wait in the tensor-core fold ran out");
+  return PPM_OK;
+}
+
 int ppm_engine_autotune(ppm_engine* e, int32_t n, const ppm_params* sample, char* report, int32_t report_len) {
   return guarded([&] {
     if (!sample || n < 1) throw Error(PPM_E_INVALID, "autotune needs sample profiles");
@@ -337,6 +347,18 @@ int ppm_engine_autotune(ppm_engine* e, int32_t n, const ppm_params* sample, char
       std::memcpy(report, r.data(), k);
       report[k] = 0;
     }
+  });
+}
+
+int ppm_fold(ppm_engine* e, int32_t response, int32_t fold, int32_t n_profiles, int32_t n_bins, const double* alpha,
+             const double* flux, double* counts) {
+  return guarded([&] { eng(e).fold(response, fold, n_profiles, n_bins, alpha, flux, counts, false, nullptr); });
+}
+
+int ppm_fold_device(ppm_engine* e, int32_t response, int32_t fold, int32_t n_profiles, int32_t n_bins,
+                    const double* alpha, const double* flux_device, double* counts_device, void* stream) {
+  return guarded([&] {
+    eng(e).fold(response, fold, n_profiles, n_bins, alpha, flux_device, counts_device, true, (cudaStream_t)stream);
   });
 }
 

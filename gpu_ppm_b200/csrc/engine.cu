@@ -1081,6 +1081,55 @@ std::string Engine::autotune(int n, const ppm_params* sample) {
   return rep;
 }
 
+// The fold of given flux arrays, the reference's matmul (gpu/matmul.cuh:12-36)
+// on its own: the same kernels as the fold stage of a pass.
+void Engine::fold(int resp, int mode, int n_prof, int n_bins, const double* alpha, const double* flux, double* counts,
+                  bool device, cudaStream_t st) {
+  NvtxRange range("ppm_fold");
+  std::lock_guard<std::mutex> lk(mu);
+  if (resp < 0 || resp >= (int)resps.size()) throw Error(PPM_E_INVALID, "unknown response");
+  if (mode < 0 || mode > 2) throw Error(PPM_E_INVALID, "unknown fold");
+  if (n_prof < 1 || n_bins < 1 || n_bins > 4096) throw Error(PPM_E_RANGE, "n_profiles >= 1 and n_bins in [1, 4096]");
+  if (!alpha || !flux || !counts) throw Error(PPM_E_INVALID, "null alpha, flux or counts");
+  if ((long long)n_prof * n_bins > (1ll << 31) / 2) throw Error(PPM_E_RANGE, "too many (profile, bin) rows");
+  PPM_CUDA(cudaSetDevice(cfg.device));
+  const Resp& r = resps[resp];
+  const size_t n_flux = (size_t)n_prof * n_bins * r.n_e, n_counts = (size_t)n_prof * n_bins * r.n_ch;
+  std::vector<FoldJob> jobs(n_prof);
+  for (int j = 0; j < n_prof; ++j)
+    jobs[j] = FoldJob{(long long)j * n_bins * r.n_e, (long long)j * n_bins * r.n_ch, alpha[j]};
+  if (!st) st = stream;
+  DeviceArena mem;
+  const double* d_flux = flux;
+  double* d_counts = counts;
+  if (device) {
+    mem.stream = st;  // stream-ordered: the job list lives until the fold has read it
+  } else {
+    mem.cache = &block_cache;
+    double* f = (double*)mem.alloc(sizeof(double) * n_flux);
+    d_counts = (double*)mem.alloc(sizeof(double) * n_counts);
+    PPM_CUDA(cudaMemcpyAsync(f, flux, sizeof(double) * n_flux, cudaMemcpyHostToDevice, st));
+    d_flux = f;
+  }
+  FoldJob* d_jobs = (FoldJob*)mem.alloc(sizeof(FoldJob) * jobs.size());
+  PPM_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(FoldJob) * jobs.size(), cudaMemcpyHostToDevice, st));
+  if (mode == PPM_FOLD_BF16X3 && r.tc_ok)
+    PPM_CUDA(fold_tc_launch(r, d_jobs, n_prof, n_bins, d_flux, d_counts, st));
+  else
+    PPM_CUDA(launch_fold_simt(d_jobs, n_prof, r.d_rsp, r.n_ch, r.n_e, n_bins, d_flux, d_counts, mode != PPM_FOLD_FP32,
+                              st));
+  if (!device) {
+    PPM_CUDA(cudaMemcpyAsync(counts, d_counts, sizeof(double) * n_counts, cudaMemcpyDeviceToHost, st));
+    PPM_CUDA(cudaStreamSynchronize(st));
+    int err = 0;
+    PPM_CUDA(cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+      PPM_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+      throw Error(PPM_E_TIMEOUT, "a bounded wait in the tensor-core fold ran out");
+    }
+  }
+}
+
 void Engine::output_sizes(const ppm_params& p, int64_t* n_flux, int64_t* n_counts) const {
   validate(p);
   if (n_flux) *n_flux = (int64_t)p.n_bins * (int64_t)grids[p.energy_grid].E.size();

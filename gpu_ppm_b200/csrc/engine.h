@@ -224,7 +224,11 @@ class Engine {
   int kernels_per_pass(const BatchImpl& B) const;
   void batch_launch_timed(BatchImpl& B, cudaStream_t st, float* ms);
   void output_sizes(const ppm_params& p, int64_t* n_flux, int64_t* n_counts) const;
+  // response fold alone; host buffers (copied, waits) or device buffers (enqueued on st)
+  void fold(int resp, int mode, int n_prof, int n_bins, const double* alpha, const double* flux, double* counts,
+            bool device, cudaStream_t st);
   void profile_noalloc(const ppm_params& p, double* flux_d, double* counts_d, cudaStream_t st);
+  int profile_noalloc_result(cudaStream_t st, ppm_result_info* info);
   int add_observed(int resp, int n_bins, const double* counts);
   void batch_fit(BatchImpl& B, int obs, ppm_fit* out, cudaStream_t st);
   void profile_fit(const ppm_params& p, int obs, ppm_fit* out, ppm_result_info* info);
@@ -259,8 +263,9 @@ class Engine {
   IntegrandShape choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max, int maxe_max = 0,
                               int bins_max = 0);
   void fold_tc_prepare(Resp& r);
+  // error: word the kernel sets when a bounded wait runs out (nullptr = the engine's d_err)
   cudaError_t fold_tc_launch(const Resp& r, const FoldJob* jobs, int n_jobs, int n_bins, const double* flux,
-                             double* counts, cudaStream_t st);
+                             double* counts, cudaStream_t st, int* error = nullptr);
   void track(void* p);
 
   std::mutex mu;

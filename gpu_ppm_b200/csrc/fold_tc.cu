@@ -21,7 +21,9 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -65,8 +67,8 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
   return d;
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int i = 0; i < kWaitLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit = kWaitLimit) {
+  for (int i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
@@ -94,6 +96,9 @@ struct TcArgs {
   const double* flux;
   double* counts;
   int* error;
+  // failure-path test: > 0 issues no bulk copy and no MMA and waits at most this many
+  // polls, so the first wait runs out and the kernel reports it through *error
+  int stall_wait_limit;
 };
 
 __global__ void __launch_bounds__(128, 1) fold_tc_kernel(const TcArgs a) {
@@ -135,9 +140,11 @@ __global__ void __launch_bounds__(128, 1) fold_tc_kernel(const TcArgs a) {
     src = a.flux + a.jobs[j].flux_off + (size_t)b * a.n_e;
   }
 
+  const bool stall = a.stall_wait_limit > 0;
+  const int wait_limit = stall ? a.stall_wait_limit : kWaitLimit;
   uint32_t parity = 0;
   for (int kc = 0; kc < a.k_chunks; ++kc) {
-    if (tid == 0) {
+    if (tid == 0 && !stall) {
       const uint32_t bar = smem_u32(&bar_tma);
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(2 * A_BYTES) : "memory");
       const size_t blk = ((size_t)mt * a.k_chunks + kc) * (A_BYTES / 2);
@@ -178,7 +185,7 @@ __global__ void __launch_bounds__(128, 1) fold_tc_kernel(const TcArgs a) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
-      bool ok = s_ok && mbar_wait(smem_u32(&bar_tma), parity);
+      bool ok = s_ok && mbar_wait(smem_u32(&bar_tma), parity, wait_limit);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (ok) {
         const uint32_t ah = smem_u32(sA_hi), al = smem_u32(sA_lo), bh = smem_u32(sB_hi), bl = smem_u32(sB_lo);
@@ -206,7 +213,7 @@ __global__ void __launch_bounds__(128, 1) fold_tc_kernel(const TcArgs a) {
                        smem_u32(&bar_mma))
                    : "memory");
     }
-    if (!mbar_wait(smem_u32(&bar_mma), parity)) s_ok = 0;
+    if (!mbar_wait(smem_u32(&bar_mma), parity, wait_limit)) s_ok = 0;
     parity ^= 1u;
     __syncthreads();
     if (!s_ok) break;
@@ -237,7 +244,7 @@ __global__ void __launch_bounds__(128, 1) fold_tc_kernel(const TcArgs a) {
   } else {
     // a wait ran out: record it, give in-flight MMAs one more bounded wait, then release TMEM
     if (tid == 0) atomicExch(a.error, 1);
-    mbar_wait(smem_u32(&bar_mma), parity);
+    mbar_wait(smem_u32(&bar_mma), parity, wait_limit);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -304,7 +311,7 @@ void Engine::fold_tc_prepare(Resp& r) {
 }
 
 cudaError_t Engine::fold_tc_launch(const Resp& r, const FoldJob* jobs, int n_jobs, int n_bins, const double* flux,
-                                   double* counts, cudaStream_t st) {
+                                   double* counts, cudaStream_t st, int* error) {
   cudaError_t e = once_per_device(1, [] {
     return cudaFuncSetAttribute(fold_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
   });
@@ -320,7 +327,10 @@ cudaError_t Engine::fold_tc_launch(const Resp& r, const FoldJob* jobs, int n_job
   a.jobs = jobs;
   a.flux = flux;
   a.counts = counts;
-  a.error = d_err;
+  a.error = error ? error : d_err;
+  // PPM_FOLD_TC_STALL_TEST=<polls>: the failure-path test of the bounded waits (no copy or MMA is issued, so the
+  // first wait runs out after that many polls and the call reports PPM_E_TIMEOUT)
+  if (const char* v = std::getenv("PPM_FOLD_TC_STALL_TEST")) a.stall_wait_limit = std::max(0, std::atoi(v));
   const int rows = n_jobs * n_bins;
   dim3 grid(r.m_pad / TC_M, (rows + TC_N - 1) / TC_N);
   fold_tc_kernel<<<grid, 128, SMEM_BYTES, st>>>(a);

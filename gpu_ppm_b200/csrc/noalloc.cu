@@ -12,9 +12,17 @@
 //
 // Set-up: the first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (once per device, with that device current); make that
-// first call before any stream capture.  The array is shared by every call and
-// keeps the previous call's contents; whatever must start at zero is cleared
-// on the stream by each call, and calls that overlap on the GPU race on it.
+// first call before any stream capture.  The cached address assumes that the
+// device's primary context lives until the process exits (no
+// cudaDeviceReset in between).  The array is shared by every call and keeps
+// the previous call's contents; whatever must start at zero is cleared on the
+// stream by each call, and calls that overlap on the GPU race on it.
+//
+// The call only enqueues work.  Its own status words (the fold's bounded-wait
+// flag, the work-queue overflow flag) and diagnostic counters live in the
+// array too; ppm_profile_noalloc_result waits for the stream and reports them
+// for the last call.  The call refuses a stream that is being captured: its
+// uploads come from host memory that is released when it returns.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -53,6 +61,28 @@ void* scratch_address(int dev) {
 
 size_t up256(size_t v) { return (v + 255) / 256 * 256; }
 
+// Fixed head of the scratch array: the converted profile, the counters, the
+// work-queue control words and the status words; variable-size tables follow.
+struct ScratchHead {
+  size_t prof, stats, ctrl, status, job, end;
+};
+ScratchHead scratch_head() {
+  ScratchHead h{};
+  size_t off = 0;
+  h.prof = off;
+  off += up256(sizeof(DevProfile));
+  h.stats = off;
+  off += up256(sizeof(unsigned long long) * kStats);
+  h.ctrl = off;
+  off += up256(sizeof(int) * 16);
+  h.status = off;
+  off += up256(sizeof(int) * 4);
+  h.job = off;
+  off += up256(sizeof(FoldJob));
+  h.end = off;
+  return h;
+}
+
 }  // namespace
 
 void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts_d, cudaStream_t st) {
@@ -65,6 +95,14 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
     if (e != cudaSuccess) throw Error(PPM_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
   }
   if (!st) st = stream;
+  {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) throw Error(PPM_E_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+    if (cap != cudaStreamCaptureStatusNone)
+      throw Error(PPM_E_STATE, "ppm_profile_noalloc: the stream is being captured (the uploads come from host memory "
+                               "that is released when the call returns)");
+  }
   unsigned char* base = (unsigned char*)scratch_address(cfg.device);
 
   const Grid& gr = grids[p.energy_grid];
@@ -72,16 +110,10 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   const int N = p.n_side, nf = p.n_fine;
   const bool nsx_atm = p.atmosphere == PPM_ATM_NSX;
 
-  // layout of the scratch array
-  size_t off = 0;
-  const size_t o_prof = off;
-  off += up256(sizeof(DevProfile));
-  const size_t o_stats = off;
-  off += up256(sizeof(unsigned long long) * kStats);
-  const size_t o_ctrl = off;
-  off += up256(sizeof(int) * 16);
-  const size_t o_job = off;
-  off += up256(sizeof(FoldJob));
+  // layout of the scratch array: the fixed head, then the tables and the work queue
+  const ScratchHead hd = scratch_head();
+  size_t off = hd.end;
+  const size_t o_prof = hd.prof, o_stats = hd.stats, o_ctrl = hd.ctrl, o_status = hd.status, o_job = hd.job;
   const size_t o_ring = off;
   off += up256(sizeof(double) * 3 * 4 * (size_t)N);
   const size_t o_fine = off;
@@ -174,6 +206,7 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   ck(cudaMemsetAsync(flux_d, 0, sizeof(double) * (size_t)p.n_bins * n_e, st), "flux clear");
   ck(cudaMemsetAsync(base + o_stats, 0, sizeof(unsigned long long) * kStats, st), "counter clear");
   ck(cudaMemsetAsync(base + o_ctrl, 0, sizeof(int) * 16, st), "queue clear");
+  ck(cudaMemsetAsync(base + o_status, 0, sizeof(int) * 4, st), "status clear");
 
   int* ctrl = (int*)(base + o_ctrl);
   KernelArgs a{};
@@ -201,11 +234,45 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
     ck(cudaMemcpyAsync(base + o_job, &job, sizeof(FoldJob), cudaMemcpyHostToDevice, st), "fold job upload");
     const FoldJob* dj = (const FoldJob*)(base + o_job);
     if (p.fold == PPM_FOLD_BF16X3 && r.tc_ok)
-      ck(fold_tc_launch(r, dj, 1, p.n_bins, flux_d, counts_d, st), "fold launch");
+      ck(fold_tc_launch(r, dj, 1, p.n_bins, flux_d, counts_d, st, (int*)(base + o_status)), "fold launch");
     else
       ck(launch_fold_simt(dj, 1, r.d_rsp, r.n_ch, r.n_e, p.n_bins, flux_d, counts_d, p.fold != PPM_FOLD_FP32, st),
          "fold launch");
   }
+}
+
+// Waits for `st` and reports the last ppm_profile_noalloc call's status words
+// and counters (host stack copies only: nothing is allocated).
+int Engine::profile_noalloc_result(cudaStream_t st, ppm_result_info* info) {
+  std::lock_guard<std::mutex> lk(mu);
+  auto ck = [](cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+      throw Error(PPM_E_CUDA, std::string("ppm_profile_noalloc_result: ") + what + ": " + cudaGetErrorString(e));
+  };
+  ck(cudaSetDevice(cfg.device), "cudaSetDevice");
+  if (!st) st = stream;
+  const unsigned char* base = (const unsigned char*)scratch_address(cfg.device);
+  const ScratchHead hd = scratch_head();
+  unsigned long long stats[kStats];
+  int ctrl[16], status[4];
+  ck(cudaMemcpyAsync(stats, base + hd.stats, sizeof(stats), cudaMemcpyDeviceToHost, st), "counter read");
+  ck(cudaMemcpyAsync(ctrl, base + hd.ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, st), "queue read");
+  ck(cudaMemcpyAsync(status, base + hd.status, sizeof(status), cudaMemcpyDeviceToHost, st), "status read");
+  ck(cudaStreamSynchronize(st), "stream wait");
+  int code = PPM_OK;
+  if (ctrl[2]) code = PPM_E_RANGE;      // work-queue overflow
+  else if (status[0]) code = PPM_E_TIMEOUT;  // a bounded wait of the tensor-core fold ran out
+  if (info) {
+    info->n_active = (int64_t)(stats[0] + stats[5]);
+    info->n_rings = (int64_t)stats[1];
+    info->n_dropped_rings = (int64_t)stats[2];
+    info->n_points = (int64_t)stats[3];
+    info->n_clamped = (int64_t)stats[4];
+    info->n_active_integrated = (int64_t)stats[0];
+    info->status = code;
+    info->reserved = 0;
+  }
+  return code;
 }
 
 }  // namespace ppm

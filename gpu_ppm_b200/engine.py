@@ -92,6 +92,20 @@ class Engine:
         check(lib().ppm_profile(self.h, ctypes.byref(p), dptr(flux), dptr(counts), ctypes.byref(info)))
         return flux, counts, info
 
+    def fold(self, response, flux, alpha, mode):
+        """The response fold alone (ppm_fold): flux [n_profiles][n_bins][n_e] or [n_bins][n_e], alpha per
+        profile (exposure / n_bins in the plain form); returns counts [.., n_ch, n_bins]."""
+        f = np.ascontiguousarray(flux, dtype=np.float64)
+        one = f.ndim == 2
+        if one:
+            f = f[None]
+        n_prof, n_bins, _ = f.shape
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(alpha, dtype=np.float64), (n_prof,)))
+        n_ch = self.responses[response][1]
+        counts = np.zeros((n_prof, n_ch, n_bins))
+        check(lib().ppm_fold(self.h, response, mode, n_prof, n_bins, dptr(a), dptr(f), dptr(counts)))
+        return counts[0] if one else counts
+
     def add_observed(self, response, n_bins, counts):
         """Observed counts [n_ch][n_bins] for fit statistics (ppm_engine_add_observed)."""
         c = np.ascontiguousarray(counts, dtype=np.float64).ravel()

@@ -249,9 +249,13 @@ int ppm_batch_kernel_count(ppm_engine* e, ppm_batch* b, int32_t* n);
  * start-up, a framework whose caching allocator owns the device, or a loop
  * where cudaMalloc's implicit device synchronisation would stall other
  * streams).  No counterpart in the reference: it has no allocation-free path.
- * Enqueues one profile on `stream` (a cudaStream_t, NULL = engine stream) and
- * returns without waiting; flux_device [n_bins][n_e] (required) and
- * counts_device [n_ch][n_bins] (optional) are caller-owned device buffers.
+ * Enqueues one profile on `stream` (a cudaStream_t, NULL = engine stream)
+ * without waiting for it to finish (its few small uploads come from pageable
+ * host memory, so CUDA may first wait for earlier work on that stream);
+ * flux_device [n_bins][n_e] (required) and counts_device [n_ch][n_bins]
+ * (optional) are caller-owned device buffers.  A stream that is being
+ * captured is refused with PPM_E_STATE: the uploads' host memory is released
+ * when the call returns.
  * All other working state lives in one 1 MiB device array that the library
  * declares statically (held on every device that loads the library until
  * process exit); profiles whose tables and work queue do not fit — about
@@ -259,6 +263,13 @@ int ppm_batch_kernel_count(ppm_engine* e, ppm_batch* b, int32_t* n);
  * on a device looks up the array's address; make it before any stream capture.
  * Calls share the array, so calls that overlap on the GPU race. */
 int ppm_profile_noalloc(ppm_engine* e, const ppm_params* p, double* flux_device, double* counts_device, void* stream);
+/* Outcome of the last ppm_profile_noalloc call: waits for `stream` (NULL =
+ * engine stream), fills info (active elements, rings, phase points, clamped
+ * lookups) from the counters in the static array, and returns PPM_E_TIMEOUT if
+ * a bounded wait of its tensor-core fold ran out, PPM_E_RANGE if its work
+ * queue overflowed, else PPM_OK.  Allocates nothing.  The status belongs to
+ * that call alone: other calls of the engine neither see nor clear it. */
+int ppm_profile_noalloc_result(ppm_engine* e, void* stream, ppm_result_info* info);
 
 /* Autotuner: times candidate launch shapes of the integrand — candidate
  * elements per work tile (ring granularity), CTAs per SM the register budget
@@ -299,6 +310,20 @@ int ppm_engine_add_observed(ppm_engine* e, int32_t response, int32_t n_bins, con
 int ppm_batch_fit(ppm_engine* e, ppm_batch* b, int32_t observed_id, ppm_fit* out, void* stream);
 /* Plain form: computes one profile and returns only its fit statistics. */
 int ppm_profile_fit(ppm_engine* e, const ppm_params* p, int32_t observed_id, ppm_fit* out, ppm_result_info* info);
+
+/* The response fold on its own, for flux computed elsewhere (replaces matmul,
+ * gpu/matmul.cuh:12-36, which the reference calls after its kernel,
+ * gpu/devarshi24st_gpu.cu:469-477):
+ *   counts[j][ch][b] = alpha[j] * sum_E rsp[ch][E] flux[j][b][E]
+ * for n_profiles arrays flux[j] of [n_bins][n_e] (n_e of the response's grid),
+ * with the arithmetic `fold` (PPM_FOLD_*).  alpha is per profile (the plain
+ * form uses exposure / n_bins).  ppm_fold takes host arrays and waits;
+ * ppm_fold_device takes device arrays and enqueues on `stream` (NULL = engine
+ * stream) without waiting. */
+int ppm_fold(ppm_engine* e, int32_t response, int32_t fold, int32_t n_profiles, int32_t n_bins, const double* alpha,
+             const double* flux, double* counts);
+int ppm_fold_device(ppm_engine* e, int32_t response, int32_t fold, int32_t n_profiles, int32_t n_bins,
+                    const double* alpha, const double* flux_device, double* counts_device, void* stream);
 
 /* Sizes of the output arrays for a parameter set (doubles). */
 int ppm_output_sizes(ppm_engine* e, const ppm_params* p, int64_t* n_flux, int64_t* n_counts);

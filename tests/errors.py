@@ -25,3 +25,19 @@ def max_rel(a, ref, floor=FLOOR):
 
 def median_rel(a, ref, floor=FLOOR):
     return float(np.median(rel_errors(a, ref, floor)))
+
+
+def per_channel(counts, ref, floor=FLOOR):
+    """Relative errors of counts [n_ch][n_bins] per channel, with the floor taken
+    over the whole array: (max over bins, median over bins), one entry per channel."""
+    n_ch = np.asarray(ref).shape[0]
+    e = rel_errors(counts, ref, floor).reshape(n_ch, -1)
+    return e.max(axis=1), np.median(e, axis=1)
+
+
+def per_channel_summary(counts, ref, floor=FLOOR):
+    """Distribution over channels of the per-channel max and median relative error."""
+    mx, md = per_channel(counts, ref, floor)
+    return {"channels": int(mx.size), "max_of_channel_max": float(mx.max()),
+            "median_of_channel_max": float(np.median(mx)), "max_of_channel_median": float(md.max()),
+            "median_of_channel_median": float(np.median(md))}

@@ -50,3 +50,13 @@ def test_choose_sample_respects_budget_and_spreads():
 
 def test_cpu_model_is_reported():
     assert isinstance(bench.cpu_model(), str) and bench.cpu_model()
+
+
+def test_sustainable_rate_is_the_highest_rate_kept_up_with_under_the_bound():
+    def run(rate, thr, p99):
+        return {"offered_req_per_s": rate, "throughput_req_per_s": thr, "p50_ms": 1.0, "p99_ms": p99}
+
+    curve = [run(100, 99, 5), run(500, 495, 12), run(1000, 980, 40), run(1500, 1200, 30), run(2000, 1190, 280)]
+    assert bench.sustainable(curve, 50.0)["offered_req_per_s"] == 1000  # 1500 is not kept up with
+    assert bench.sustainable(curve, 10.0)["offered_req_per_s"] == 100
+    assert bench.sustainable(curve, 1.0) is None

@@ -1,5 +1,7 @@
 """Pins the FP64 oracle against golden vectors produced by the reference's own
 CPU programs (tests/golden/make_golden.py)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -54,3 +56,21 @@ def test_tinterp_all_interpolators(golden, ora):
         flux, _ = ora.profile(p, e)
         ref = z["tinterp/" + s[0]]
         assert rel_err(flux[r0:r1:rs, c0:c1:cs], ref) < 2e-9, s[0]
+
+
+def test_config_size_fixture_inputs_rebuild():
+    """The full-size configuration fixture (tests/golden/make_config_golden.py)
+    was computed from the inputs this checkout rebuilds: same tables, grid,
+    responses and parameter structs."""
+    from tests.golden import make_config_golden as mcg
+
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "config_sizes_oracle.npz"))
+    fp = mcg.fingerprint(*mcg.inputs())
+    for k, v in fp.items():
+        if k in ("p2", "p3"):
+            assert np.array_equal(v, z["fp_" + k]), k
+        else:
+            assert np.allclose(v, z["fp_" + k], rtol=1e-12, atol=0), k
+    for name in ("config2", "config3"):
+        flux = z[name + "_flux"]
+        assert np.all(np.isfinite(flux)) and flux.max() > 0

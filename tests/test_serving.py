@@ -28,20 +28,45 @@ def served():
     e.close()
 
 
-def mixed_requests(grids, n, seed):
+def mixed_requests(grids, n, seed, n_sides=(16, 32, 48, 64), bins=(16, 32)):
     rng = np.random.default_rng(seed)
     out = []
     base, _ = synth.draw_prior(n, seed=seed, lens_u=(0.15, 0.55))
     for p in base:
         ne = int(rng.choice([128, 300]))
         g, rs = grids[ne]
-        p.n_side = int(rng.choice([16, 32, 48, 64]))
-        p.n_bins = int(rng.choice([16, 32]))
+        p.n_side = int(rng.choice(n_sides))
+        p.n_bins = int(rng.choice(bins))
         p.n_fine = 6 * p.n_bins
         p.energy_grid = g
         p.response = rs[int(rng.choice([300, 1500]))]
         out.append(p)
     return out
+
+
+def submit_all(e, reqs):
+    bufs, tickets = [], []
+    for p in reqs:
+        (fs, cs) = e.sizes(p)
+        flux, counts = np.zeros(fs), np.zeros(cs)
+        bufs.append((flux, counts))
+        tickets.append(e.submit(p, flux, counts))
+    for t in tickets:
+        assert e.wait(t, timeout_ms=120000).status == 0
+        e.release(t)
+    return bufs
+
+
+def test_large_requests_mix_equals_alone(served):
+    """Served requests at the serving workload's larger sizes (N_side 256 / 512,
+    64 / 128 bins, both energy grids and responses) equal the profile alone."""
+    e, grids = served
+    reqs = mixed_requests(grids, 12, seed=21, n_sides=(256, 512), bins=(64, 128))
+    bufs = submit_all(e, reqs)
+    for p, (flux, counts) in zip(reqs, bufs):
+        f1, c1, _ = e.profile(p)
+        assert max_rel(flux, f1) < 1e-5, (p.n_side, p.n_bins)
+        assert max_rel(counts, c1) < 1e-5, (p.n_side, p.n_bins)
 
 
 def test_mix_equals_alone_and_latency_reported(served):
