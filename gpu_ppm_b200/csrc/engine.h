@@ -87,11 +87,12 @@ struct Resp {
   int grid = 0, n_ch = 0, n_e = 0;
   double* d_rsp = nullptr;
   std::vector<double> h_rsp;
-  // tensor-core fold operands: BF16 hi/lo split of rsp, zero padded, in the UMMA core-matrix layout
+  // tensor-core fold operands: BF16 hi/lo split of rsp, zero padded, in the UMMA core-matrix layout,
+  // one block per (channel group, 32-energy chunk)
   bool tc_ok = false;
-  int m_pad = 0, k_pad = 0;
-  void* d_a_hi = nullptr;
-  void* d_a_lo = nullptr;
+  int tc_groups = 0, tc_ng = 0, tc_k_chunks = 0;
+  void* d_b_hi = nullptr;
+  void* d_b_lo = nullptr;
 };
 
 // Device allocations owned by one batch.
