@@ -553,7 +553,7 @@ def random_walk_requests(n, seed, grids, synth, abi):
     return out
 
 
-SERVE_RATES = ((100.0, 200), (250.0, 300), (500.0, 400), (750.0, 500), (1000.0, 600), (1500.0, 700), (2000.0, 800))
+SERVE_RATES = tuple((r, 600) for r in (100.0, 250.0, 500.0, 750.0, 1000.0, 1500.0, 2000.0, 3000.0))
 SERVE_P99_BOUND_MS = 50.0  # the latency bound the sustainable rate is stated against
 
 
@@ -583,8 +583,10 @@ def serving_bench(lens, nsx, synth, abi, Engine, device, rates=SERVE_RATES):
     for t in [eng.submit(p, None, b) for p, b in zip(warm, bufs)]:
         eng.wait(t)
         eng.release(t)
+    # one request stream for every offered rate (the same sampler walk, so the rates see the same request mix)
+    stream_reqs = random_walk_requests(max(n for _, n in rates), 1000, grids, synth, abi)
     for k, (rate, n) in enumerate(rates):
-        reqs = random_walk_requests(n, 1000 + k, grids, synth, abi)
+        reqs = stream_reqs[:n]
         rng = np.random.default_rng(k)
         t_arr = np.cumsum(rng.exponential(1.0 / rate, size=n))
         bufs, tickets, lag, sub = [], [], [], []

@@ -37,6 +37,7 @@ namespace {
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kTwoPi = 2. * kPi;
 constexpr int kSlotBytes = 48;  // bytes per batch point (SoA)
+constexpr int kPhaseMajorMaxE = 4;  // blackbody grids of at most this many energies take the phase-major walk
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
@@ -1020,6 +1021,74 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
       const int n_fp = n_fine + 1;
       const double P0 = s.P[0];
       const Real inv_kT = (Real)1 / kT;
+      if (n_e <= kPhaseMajorMaxE && staged && mono) {
+        // Phase-major walk (the os1 light curves: one energy).  A work item is
+        // one phase point and a contiguous segment of the tile's active
+        // elements.  The elements' azimuths increase along the ring, so the
+        // point's patch phase moves monotonically from one element to the
+        // next (wrapping once past 1) and its phase_o bracket is hunted from
+        // the previous element's: vhunt's bracket exactly, as phase_o is
+        // non-decreasing.  The point's sums stay in FP64 registers; one atomic
+        // per energy flushes them at the end of the segment.
+        const int n_gl = p.n_gl;
+        const double inv_bins = 1. / p.n_bins;
+        const int segs = max(1, min(n_act, nt / max(1, n_pp)));
+        const int n_items = n_pp * segs;
+        const double scale = out_scale;
+        unsigned int n_vis = 0;
+        for (int it = tid; it < n_items; it += nt) {
+          const int k = it % n_pp, seg = it / n_pp;
+          const int jj0 = (int)((long long)n_act * seg / segs), jj1 = (int)((long long)n_act * (seg + 1) / segs);
+          int bin, g = 0;
+          if (n_gl > 0) {
+            bin = k / n_gl;
+            g = k - bin * n_gl;
+          } else {
+            bin = k;
+          }
+          double ppt, wgl;
+          if (n_gl > 0) {
+            const double lb = bin * inv_bins, ub = (bin + 1) * inv_bins;
+            ppt = 0.5 * (lb + ub + c_gl_nodes[n_gl * (n_gl - 1) / 2 + g] * (ub - lb));
+            wgl = 0.5 * 1. * c_gl_weights[n_gl * (n_gl - 1) / 2 + g];
+          } else {
+            ppt = bin * inv_bins;
+            wgl = 1.0;
+          }
+          double acc[kPhaseMajorMaxE];
+#pragma unroll
+          for (int e = 0; e < kPhaseMajorMaxE; ++e) acc[e] = 0.0;
+          int hint = -1;
+          for (int jj = jj0; jj < jj1; ++jj) {
+            const double phase_shift = (point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs)) / kTwoPi;
+            const double xph = ppt + phase_shift + 1.;
+            double patch = xph - floor(xph);
+            if (patch < P0) patch += 1.;
+            hint = hunt_from(s.P, n_fp, patch, hint);
+            const int i = clampi(hint, 0, n_fp - 2);
+            const double af = (patch - s.P[i]) * inv_dp[i];
+            const double flux = (1 - af) * s.F[i] + af * s.F[i + 1];
+            if (flux == 0) continue;
+            const double z = (1 - af) * s.Z[i] + af * s.Z[i + 1];
+            ++n_vis;
+            const Real cb = (Real)(flux * wgl), zb = (Real)z;
+#pragma unroll
+            for (int e = 0; e < kPhaseMajorMaxE; ++e)
+              if (e < n_e) {
+                const Real Ee = E_s[e] * zb;
+                acc[e] += (double)(cb * (Ee * Ee * Ee / expm1(Ee * inv_kT)));  // Ibb without its constant
+              }
+          }
+#pragma unroll
+          for (int e = 0; e < kPhaseMajorMaxE; ++e)
+            if (e < n_e && acc[e] != 0.0) atomicAdd(flux_base + (size_t)bin * n_e + e, acc[e] * scale * invE_s[e]);
+        }
+        const int lane = tid & 31;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) n_vis += __shfl_down_sync(0xffffffffu, n_vis, off);
+        if (lane == 0 && n_vis) atomicAdd(&p.stats[3], (unsigned long long)n_vis);
+        continue;
+      }
       const int runs = max(1, min(n_pp, nt / n_act));  // runs of phase points per element
       const int per_run = (n_pp + runs - 1) / runs;
       const int n_items = n_act * runs;
