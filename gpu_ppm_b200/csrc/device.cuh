@@ -80,17 +80,38 @@ struct DevProfile {
   const double* fine;   // [n_fine] (cos 2 pi k/n, sin 2 pi k/n)
   DevGrid grid;
   unsigned long long* stats;  // [kStats]
+  unsigned* ring_seen;        // [kMaxSpots][ring_words] bits: rings already counted in stats[1]
+  int ring_words;
   DevSpot spot[kMaxSpots];
 };
 
-// One unit of work: candidate elements j in [j0, j1) of one ring of one spot.
+// One unit of work: candidate elements j in [j0, j1) of one ring of one spot,
+// at the phase nodes u in [u0, u1) (u = bin * max(n_gl, 1) + GL point).
 struct Tile {
   int profile;
   short spot;
   short first;  // 1 for the first chunk of a ring
   int ring;     // HEALPix ring index (1..4N-1), 0 for a point source
   int j0, j1;
+  short u0, u1;
 };
+
+// Adds v to *a with a compensated (TwoSum) accumulation: the atomic returns the
+// old value, so the rounding error of old + v is known exactly and is added to
+// the compensation pool *c.  *a + *c is then the sum of every value added, to
+// within a rounding of the compensation itself (about 1e-32 relative), in any
+// order of the additions.  Without a pool (c == nullptr) a plain atomic add.
+__device__ __forceinline__ void comp_add(double* a, double* c, double v) {
+  if (!c) {
+    atomicAdd(a, v);
+    return;
+  }
+  const double old = atomicAdd(a, v);
+  const double s = old + v;
+  const double bb = s - old;
+  const double err = (old - (s - bb)) + (v - bb);
+  if (err != 0.0) atomicAdd(c, err);
+}
 
 struct WorkQueue {
   Tile* tiles;

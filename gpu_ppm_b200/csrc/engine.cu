@@ -657,24 +657,35 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
     const long long nc = ps[i].response >= 0 ? (long long)resps[ps[i].response].n_ch * ps[i].n_bins : 0;
     B.counts_off[i + 1] = B.counts_off[i] + nc;
   }
-  // kernel variants: 0 = NSX, 1 = blackbody FP64, 2 = blackbody FP32
-  auto variant = [](const ppm_params& p) {
-    return p.atmosphere == PPM_ATM_NSX ? 0 : (p.precision == PPM_PREC_FP64 ? 1 : 2);
+  // kernel variants, one group and integrand launch each: 0 = NSX home-cell kernel, 1 = blackbody FP64,
+  // 2 = blackbody FP32, 3 = NSX pooled-polynomial kernel (grids the home-cell kernel does not take)
+  std::map<int, bool> cell_ok;  // per energy grid
+  auto variant = [&](const ppm_params& p) -> int {
+    if (p.atmosphere != PPM_ATM_NSX) return p.precision == PPM_PREC_FP64 ? 1 : 2;
+    auto it = cell_ok.find(p.energy_grid);
+    if (it == cell_ok.end()) it = cell_ok.emplace(p.energy_grid, cell_kernel_takes(p.energy_grid)).first;
+    return it->second ? 0 : 3;
   };
-  std::vector<int> order;
+  constexpr int NV = 4;
+  std::vector<int> order, vof(n);
   order.reserve(n);
-  for (int v = 0; v < 3; ++v)
+  for (int i = 0; i < n; ++i) vof[i] = variant(ps[i]);
+  for (int v = 0; v < NV; ++v)
     for (int i = 0; i < n; ++i)
-      if (variant(ps[i]) == v) order.push_back(i);
+      if (vof[i] == v) order.push_back(i);
   B.d_stats = (unsigned long long*)B.mem.alloc(sizeof(unsigned long long) * kStats * (size_t)n);
+  // ring bits per profile and spot (rings 0 .. 4 N_side - 1)
+  std::vector<long long> ring_off(n + 1, 0);
+  for (int i = 0; i < n; ++i) ring_off[i + 1] = ring_off[i] + (long long)kMaxSpots * (4ll * ps[i].n_side / 32 + 1);
+  B.ring_words = ring_off[n];
+  B.d_ring_seen = (unsigned*)B.mem.alloc(sizeof(unsigned) * (size_t)B.ring_words);
   std::vector<DevProfile> hp(n);
-  long long cap[3] = {0, 0, 0};
-  int start[4] = {0, 0, 0, 0};
-  double work = 0;     // phase points of the batch, estimated from the spots' areas
-  long long pts_max = 1;  // phase points per element, largest profile
+  GroupWork gw[NV];
   for (int k = 0; k < n; ++k) {
     const int i = order[k];
     to_device(ps[i], hp[k], B.flux_off[i], B.d_stats + (size_t)kStats * i);
+    hp[k].ring_seen = B.d_ring_seen + ring_off[i];
+    hp[k].ring_words = (int)(4ll * ps[i].n_side / 32 + 1);
     for (int s = 0; s < ps[i].n_spots; ++s) {  // ring window (a point source is ring 0)
       DevSpot& sp = hp[k].spot[s];
       if (sp.kind == PPM_SPOT_POINT) {
@@ -687,31 +698,26 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
         sp.i_hi = std::min(sp.i_hi, ring_end - 1);
       }
     }
-    const long long pts = (long long)ps[i].n_bins * std::max(1, ps[i].n_gl);
-    pts_max = std::max(pts_max, pts);
-    work += spot_elements(ps[i]) * (double)pts;
+    gw[vof[i]].add(ps[i], hp[k]);
   }
-  const int chunk = chunk_override > 0 ? chunk_override : tile_chunk(work, pts_max);
-  B.chunk = chunk;
+  int chunk[NV], npt[NV];
+  for (int v = 0; v < NV; ++v) group_tiling(v == 3, gw[v], chunk_override, &chunk[v], &npt[v]);
+  B.chunk = chunk[0];
+  long long cap[NV] = {0, 0, 0, 0};
+  int start[NV + 1] = {0, 0, 0, 0, 0};
   for (int k = 0; k < n; ++k) {
     const int i = order[k];
-    const int v = variant(ps[i]);
-    for (int s = 0; s < ps[i].n_spots; ++s) {
-      const DevSpot& sp = hp[k].spot[s];
-      if (sp.kind == PPM_SPOT_POINT) {
-        cap[v] += sp.i_hi >= sp.i_lo ? 1 : 0;
-      } else if (sp.i_hi >= sp.i_lo) {
-        const long long rings = sp.i_hi - sp.i_lo + 1;
-        cap[v] += rings * (2 + (4ll * ps[i].n_side + chunk - 1) / chunk);
-      }
-    }
+    const int v = vof[i];
+    cap[v] += tile_bound(ps[i], hp[k], chunk[v], npt[v]);
     start[v + 1] = k + 1;
   }
-  for (int v = 1; v <= 3; ++v) start[v] = std::max(start[v], start[v - 1]);
-  const long long cap_total = cap[0] + cap[1] + cap[2];
+  for (int v = 1; v <= NV; ++v) start[v] = std::max(start[v], start[v - 1]);
+  long long cap_total = 0;
+  for (int v = 0; v < NV; ++v) cap_total += cap[v];
   if (cap_total > (1ll << 31) - 1) throw Error(PPM_E_RANGE, "batch too large for one work queue");
   B.d_prof = (DevProfile*)B.mem.alloc(sizeof(DevProfile) * (size_t)n);
   B.d_flux = (double*)B.mem.alloc(sizeof(double) * (size_t)std::max(1ll, B.flux_off[n]));
+  B.d_comp = (double*)B.mem.alloc(sizeof(double) * (size_t)std::max(1ll, B.flux_off[n]));
   B.d_counts = (double*)B.mem.alloc(sizeof(double) * (size_t)std::max(1ll, B.counts_off[n]));
   Tile* tiles = (Tile*)B.mem.alloc(sizeof(Tile) * (size_t)std::max(1ll, cap_total));
   B.d_ctrl = (int*)B.mem.alloc(sizeof(int) * 16);
@@ -722,12 +728,14 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
   B.h2d_bytes = sizeof(DevProfile) * (size_t)n;
   long long base = 0;
   B.groups.clear();
-  for (int v = 0; v < 3; ++v) {
+  for (int v = 0; v < NV; ++v) {
     const int g0 = start[v], g1 = start[v + 1];
     if (g1 <= g0) continue;
     BatchImpl::Group G;
     G.g0 = g0;
     G.g1 = g1;
+    G.chunk = chunk[v];
+    G.npt = npt[v];
     WorkQueue& q = G.args.queue;
     q.tiles = tiles + base;
     q.capacity = (int)cap[v];
@@ -747,7 +755,9 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
     G.args.lens = lens;
     G.args.nsx = nsx;
     G.args.flux = B.d_flux;
-    G.args.shape = choose_shape(v == 0, v == 1, ne_max, nf_max, cells_max, maxe_max, bins_max);
+    G.args.comp = B.d_comp;
+    G.args.shape = choose_shape(v == 0 || v == 3, v == 1, ne_max, nf_max, cells_max, maxe_max, bins_max, v == 0);
+    if (v == 0 && !G.args.shape.cellk) throw Error(PPM_E_STATE, "home-cell NSX kernel expected for the grid");
     PPM_CUDA(configure_integrand_smem(G.args.shape));
     const int occ = max_active_ctas(G.args.shape);
     if (occ < 1)
@@ -790,14 +800,19 @@ void Engine::batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events) {
   {
     NvtxRange range("clear + plan");
     PPM_CUDA(cudaMemsetAsync(B.d_flux, 0, sizeof(double) * (size_t)B.flux_off[n], st));
+    PPM_CUDA(cudaMemsetAsync(B.d_comp, 0, sizeof(double) * (size_t)B.flux_off[n], st));
     PPM_CUDA(cudaMemsetAsync(B.d_stats, 0, sizeof(unsigned long long) * kStats * (size_t)n, st));
+    PPM_CUDA(cudaMemsetAsync(B.d_ring_seen, 0, sizeof(unsigned) * (size_t)B.ring_words, st));
     PPM_CUDA(cudaMemsetAsync(B.d_ctrl, 0, sizeof(int) * 16, st));
-    for (const auto& G : B.groups) PPM_CUDA(launch_plan(B.d_prof + G.g0, G.g1 - G.g0, lens, G.args.queue, B.chunk, st));
+    for (const auto& G : B.groups)
+      PPM_CUDA(launch_plan(B.d_prof + G.g0, G.g1 - G.g0, lens, G.args.queue, G.chunk, G.npt, st));
   }
   if (events) PPM_CUDA(cudaEventRecord(events[1], st));
   {
     NvtxRange range("integrand");
     for (const auto& G : B.groups) PPM_CUDA(launch_integrand(G.args, G.grid, st));
+    // the compensation pool's rounding errors back into the flux pool
+    PPM_CUDA(launch_add_comp(B.d_flux, B.d_comp, B.flux_off[n], sm_count, st));
   }
   if (events) PPM_CUDA(cudaEventRecord(events[2], st));
   NvtxRange fold_range("fold");
@@ -823,7 +838,9 @@ void Engine::batch_launch_timed(BatchImpl& B, cudaStream_t st, float* ms) {
   for (int k = 0; k < 3; ++k) PPM_CUDA(cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]));
 }
 
-int Engine::kernels_per_pass(const BatchImpl& B) const { return 2 * (int)B.groups.size() + (int)B.folds.size(); }
+int Engine::kernels_per_pass(const BatchImpl& B) const {
+  return 2 * (int)B.groups.size() + 1 + (int)B.folds.size();  // plan + integrand per group, add_comp, folds
+}
 
 void Engine::batch_capture(BatchImpl& B) {
   cudaStream_t cs;
@@ -872,7 +889,7 @@ void Engine::batch_collect(BatchImpl& B, double* flux, double* counts, ppm_resul
   PPM_CUDA(cudaMemcpyAsync(ctrl, B.d_ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, st));
   PPM_CUDA(cudaStreamSynchronize(st));
   PPM_CUDA(cudaGetLastError());
-  if (ctrl[2] || ctrl[5] || ctrl[8]) throw Error(PPM_E_RANGE, "work queue overflow");
+  if (ctrl[2] || ctrl[5] || ctrl[8] || ctrl[11]) throw Error(PPM_E_RANGE, "work queue overflow");
   int err = 0;
   PPM_CUDA(cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) {
@@ -929,6 +946,64 @@ int Engine::tile_chunk(double work, long long pts_max) const {
   return std::max(c, std::min(tune.chunk, tune.small_chunk));
 }
 
+void GroupWork::add(const ppm_params& p, const DevProfile& d) {
+  const long long pts = (long long)p.n_bins * std::max(1, p.n_gl);
+  pts_max = std::max(pts_max, pts);
+  nodes_max = std::max(nodes_max, (int)pts);
+  work += Engine::spot_elements(p) * (double)pts;
+  for (int s = 0; s < p.n_spots; ++s) {
+    const DevSpot& sp = d.spot[s];
+    if (sp.kind == PPM_SPOT_POINT)
+      rings += sp.i_hi >= sp.i_lo ? 1 : 0;
+    else if (sp.i_hi >= sp.i_lo)
+      rings += sp.i_hi - sp.i_lo + 1;
+  }
+}
+
+// Tiling of one kernel group.  The home-cell NSX and the blackbody kernels
+// keep the tuned element chunk in every batch, so that a profile's tiles cover
+// the same elements alone and in any batch; a batch with few rings is spread
+// over the SMs by splitting each tile's phase nodes instead (about 8 tiles per
+// CTA slot, at least kMinNodesPerTile nodes per tile).  The pooled kernel
+// splits the elements (tile_chunk) and takes all nodes.
+void Engine::group_tiling(bool pooled, const GroupWork& w, int chunk_override, int* chunk, int* npt) const {
+  if (pooled) {
+    *chunk = chunk_override > 0 ? chunk_override : tile_chunk(w.work, w.pts_max);
+    *npt = 0;
+    return;
+  }
+  *chunk = chunk_override > 0 ? chunk_override : tune.chunk;
+  const double want = 8.0 * sm_count * 3;
+  const double splits_d = std::ceil(want / std::max<double>(1.0, (double)w.rings));
+  const int max_splits = std::max(1, w.nodes_max / kMinNodesPerTile);
+  const int splits = (int)std::max(1.0, std::min<double>(splits_d, max_splits));
+  *npt = splits <= 1 ? 0 : (w.nodes_max + splits - 1) / splits;
+}
+
+// Work tiles the planner may push for one profile (its queue capacity).
+long long Engine::tile_bound(const ppm_params& p, const DevProfile& d, int chunk, int npt) const {
+  const int nodes = p.n_bins * std::max(1, p.n_gl);
+  const long long per = npt > 0 ? (nodes + npt - 1) / npt : 1;
+  long long cap = 0;
+  for (int s = 0; s < p.n_spots; ++s) {
+    const DevSpot& sp = d.spot[s];
+    if (sp.kind == PPM_SPOT_POINT)
+      cap += sp.i_hi >= sp.i_lo ? per : 0;
+    else if (sp.i_hi >= sp.i_lo)
+      cap += (long long)(sp.i_hi - sp.i_lo + 1) * (2 + (4ll * p.n_side + chunk - 1) / chunk) * per;
+  }
+  return cap;
+}
+
+// Whether the home-cell NSX kernel takes profiles on this energy grid.
+bool Engine::cell_kernel_takes(int grid) {
+  if (tune.kernel != 0 || !has_nsx) return false;
+  prepare_grid(grid);
+  const Grid& g = grids[grid];
+  const IntegrandShape s = choose_shape(true, false, (int)g.E.size(), 2, g.span + 1, g.maxe, 1, true);
+  return s.cellk != 0;
+}
+
 void Engine::profile_rings(const ppm_params& p, int ring_begin, int ring_end, double* flux, double* counts,
                            ppm_result_info* info) {
   std::lock_guard<std::mutex> lk(mu);
@@ -951,13 +1026,13 @@ void Engine::profile_batch(int n, const ppm_params* ps, double* flux, double* co
 }
 
 IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max, int maxe_max,
-                                    int bins_max) {
+                                    int bins_max, bool allow_cell) {
   // home-cell NSX kernel: cpl cells per lane (the last (cpl + 3) / cpl lanes of a warp
   // only supply slice rows), warp sets up to 512 threads
   const int span_max = cells_max - 1;
   const int maxe_t = maxe_max <= 4 ? 4 : (maxe_max <= 8 ? 8 : 16);
-  if (nsx_kernel && tune.kernel == 0 && maxe_max >= 1 && maxe_max <= 16 && span_max <= 16 * 32 && nsx.nmu < 4096 &&
-      bins_max < (1 << 20)) {
+  if (allow_cell && nsx_kernel && tune.kernel == 0 && maxe_max >= 1 && maxe_max <= 16 && span_max <= 16 * 32 &&
+      nsx.nmu < 4096 && bins_max < (1 << 20)) {
     // cells per lane: fewest estimated lane instructions per point (window rows,
     // polynomials, record handling, energy slots), over what the slots' registers allow
     const int cmax = maxe_t == 4 ? 3 : (maxe_t == 8 ? 2 : 1);

@@ -138,12 +138,16 @@ struct BatchImpl {
   DeviceArena mem;
   DevProfile* d_prof = nullptr;
   double* d_flux = nullptr;
+  double* d_comp = nullptr;       // compensation pool of the flux pool's atomic additions
   double* d_counts = nullptr;
+  unsigned* d_ring_seen = nullptr;  // ring bits behind the rings-with-active-elements counter
+  long long ring_words = 0;
   unsigned long long* d_stats = nullptr;
   int* d_ctrl = nullptr;
   FoldJob* d_jobs = nullptr;
   struct Group {
     int g0 = 0, g1 = 0, grid = 0;
+    int chunk = 1024, npt = 0;  // candidate elements and phase nodes (0 = all) per tile
     KernelArgs args{};
   };
   struct Fold {
@@ -154,7 +158,7 @@ struct BatchImpl {
   size_t h2d_bytes = 0;
   cudaGraphExec_t graph = nullptr;
   cudaStream_t last_stream = nullptr;
-  int chunk = 1024;                // candidate elements per tile of this batch
+  int chunk = 1024;                // candidate elements per tile of the home-cell NSX group
   long long* d_fit_off = nullptr;  // counts offset per profile (fit statistics)
   ppm_fit* d_fit = nullptr;
   BatchImpl() = default;
@@ -172,6 +176,16 @@ struct GridSplit {
   double lo = 0, hi = 0;
 };
 void split_grid(const std::vector<double>& E, double inv_dE, GridSplit& out);
+
+// Work estimate of one kernel group of a batch (the tiling's inputs).
+constexpr int kMinNodesPerTile = 8;
+struct GroupWork {
+  double work = 0;        // phase points, estimated from the spots' areas
+  long long pts_max = 1;  // phase points per element, largest profile
+  long long rings = 0;    // rings that may hold active elements
+  int nodes_max = 1;      // phase nodes per profile, largest profile
+  void add(const ppm_params& p, const DevProfile& d);
+};
 
 struct Tuning {
   int pb = 20;       // phase points per polynomial sub-batch (rounded to whole warps)
@@ -262,7 +276,10 @@ class Engine {
   const double* ring_table(int N);
   const double* fine_table(int nf);
   IntegrandShape choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max, int maxe_max = 0,
-                              int bins_max = 0);
+                              int bins_max = 0, bool allow_cell = true);
+  bool cell_kernel_takes(int grid);
+  void group_tiling(bool pooled, const GroupWork& w, int chunk_override, int* chunk, int* npt) const;
+  long long tile_bound(const ppm_params& p, const DevProfile& d, int chunk, int npt) const;
   void fold_tc_prepare(Resp& r);
   // error: word the kernel sets when a bounded wait runs out (nullptr = the engine's d_err)
   cudaError_t fold_tc_launch(const Resp& r, const FoldJob* jobs, int n_jobs, int n_bins, const double* flux,

@@ -128,9 +128,15 @@ __device__ int tile_prologue(const KernelArgs& a, const DevProfile& p, const Dev
   __syncthreads();
   if (n_act == 0) return 0;
   if (tid == 0) {
-    atomicAdd(&p.stats[0], (unsigned long long)n_act);
-    atomicAdd(&p.stats[1], 1ull);
-    if (s_g.u_clamped && tile.first) atomicAdd(&p.stats[4], 1ull);
+    // counted by the tiles of the first node range only; a ring counts once, by the first of its tiles to
+    // find active elements
+    if (tile.u0 == 0) {
+      atomicAdd(&p.stats[0], (unsigned long long)n_act);
+      const unsigned bit = 1u << (tile.ring & 31);
+      if (!(atomicOr(&p.ring_seen[tile.spot * p.ring_words + (tile.ring >> 5)], bit) & bit))
+        atomicAdd(&p.stats[1], 1ull);
+      if (s_g.u_clamped && tile.first) atomicAdd(&p.stats[4], 1ull);
+    }
     s_int[40] = p.n_fine + 1;  // invisible min
     s_int[41] = -1;            // invisible max
   }
@@ -188,31 +194,30 @@ __device__ int tile_prologue(const KernelArgs& a, const DevProfile& p, const Dev
   return n_act;
 }
 
-// Phase point q of the tile: GL node (or sample phase), patch phase, hunt and
-// lerps in FP64 (cpu/devarshi24st_cpu.cpp:214-229).  Returns flux/I (0 = skip).
-__device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtrs& s, const RingPhi& rp, bool point,
-                                              int n_act, int q, int& bin, double& wgl, double& z, double& mu) {
+// Phase node u = bin * n_gl + GL point (u = bin when n_gl = 0): its bin, its
+// phase ppt and GL weight (cpu/devarshi24st_cpu.cpp:214-219).
+__device__ __forceinline__ void node_phase(const DevProfile& p, int u, int& bin, double& ppt, double& wgl) {
   const int n_gl = p.n_gl;
-  const int i_pp = q / n_act, jj = q - i_pp * n_act;
-  int g = 0;
   if (n_gl > 0) {
-    bin = i_pp / n_gl;
-    g = i_pp - bin * n_gl;
-  } else {
-    bin = i_pp;
-  }
-  const double phi = point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs);
-  const double phase_shift = phi / kTwoPi;
-  double ppt;
-  if (n_gl > 0) {
+    bin = u / n_gl;
+    const int g = u - bin * n_gl;
     const double width = 1. / p.n_bins;
     const double lb = bin * width, ub = (bin + 1) * width;
     ppt = 0.5 * (lb + ub + c_gl_nodes[n_gl * (n_gl - 1) / 2 + g] * (ub - lb));
     wgl = 0.5 * 1. * c_gl_weights[n_gl * (n_gl - 1) / 2 + g];
   } else {
+    bin = u;
     ppt = bin * (1.0 / p.n_bins);
     wgl = 1.0;
   }
+}
+
+// Active element jj of the tile at phase ppt: patch phase, hunt and lerps in
+// FP64 (cpu/devarshi24st_cpu.cpp:220-229).  Returns flux/I (0 = skip).
+__device__ __forceinline__ double node_point(const DevProfile& p, const SmemPtrs& s, const RingPhi& rp, bool point,
+                                             int jj, double ppt, double& z, double& mu) {
+  const double phi = point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs);
+  const double phase_shift = phi / kTwoPi;
   // fmod(x, 1) of x = ppt + phase_shift + 1 in [1, 3): x - floor(x) is the same exact value
   const double xph = ppt + phase_shift + 1.;
   double patch = xph - floor(xph);
@@ -224,6 +229,24 @@ __device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtr
   z = (1 - af) * s.Z[i] + af * s.Z[i + 1];
   mu = (1 - af) * s.MU[i] + af * s.MU[i + 1];
   return flux;
+}
+
+// Phase point q of the tile's node range (node u0 + q / n_act, element q % n_act).
+__device__ __forceinline__ double phase_point(const DevProfile& p, const SmemPtrs& s, const RingPhi& rp, bool point,
+                                              int n_act, int u0, int q, int& bin, double& wgl, double& z, double& mu) {
+  const int du = q / n_act, jj = q - du * n_act;
+  double ppt;
+  node_phase(p, u0 + du, bin, ppt, wgl);
+  return node_point(p, s, rp, point, jj, ppt, z, mu);
+}
+
+// Barrier of one warp set of n threads (a multiple of 32): the warp itself for
+// a one-warp set, else named barrier 1 + set.
+__device__ __forceinline__ void set_sync(int set, int n) {
+  if (n == 32)
+    __syncwarp();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + set), "r"(n) : "memory");
 }
 
 // phase_point's arithmetic for one element at phase point i_pp, for the
@@ -376,18 +399,21 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 320, MINB) integrand_nsx_ker
     const bool cubicE = mode != 4;
     const bool sg = mode == 1;
     const double mu_min = s.mu[nmu - 1];
-    const int n_pp = p.n_gl > 0 ? p.n_bins * p.n_gl : p.n_bins;
+    const int n_pp = tile.u1 - tile.u0;  // the tile's phase nodes
     const int n_pts = n_pp * n_act;
     int cur_bin = -1;
     double* flux_base = a.flux + p.flux_off;
     const double out_scale = sp.out_scale;
 
+    double* comp_base = a.comp ? a.comp + p.flux_off : nullptr;
     auto flush = [&]() {
 #pragma unroll
       for (int k = 0; k < NE_T; ++k) {
         const int e = tid + k * nt;
-        if (e < n_e && acc[k] != 0.f)
-          atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)acc[k] * out_scale * G.invE[e]);
+        if (e < n_e && acc[k] != 0.f) {
+          const size_t o = (size_t)cur_bin * n_e + e;
+          comp_add(flux_base + o, comp_base ? comp_base + o : nullptr, (double)acc[k] * out_scale * G.invE[e]);
+        }
         acc[k] = 0.f;
       }
     };
@@ -404,7 +430,7 @@ __global__ void __launch_bounds__(MINB == 1 ? 512 : 320, MINB) integrand_nsx_ker
       const int q = q0 + tid;
       if (q < n_pts) {
         double wgl, z = 0, mu = 0;
-        const double flux = phase_point(p, s, rp, point, n_act, q, bin, wgl, z, mu);
+        const double flux = phase_point(p, s, rp, point, n_act, tile.u0, q, bin, wgl, z, mu);
         if (flux != 0.0) {
           vis = true;
           if (mu < mu_min) mu = mu_min;
@@ -677,6 +703,10 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
   __shared__ float s_tapw[16];
   __shared__ int s_tapo[16];
   __shared__ int s_ntap;
+  __shared__ int s_node[16], s_bin[16];          // node taken by each warp set, its bin
+  __shared__ double s_ppt[16], s_wgl[16];        // the node's phase and GL weight
+  __shared__ int s_wcnt[16];                     // visible points per warp (sets of several warps)
+  __shared__ unsigned s_nvis[16], s_nclamp[16];  // per warp: visible and clamped points of the tile
   const int tid = threadIdx.x, nt = blockDim.x;
   const DevNsx& X = a.nsx;
   const int nE = X.nE, nmu = X.nmu, ldS = S.ldS;
@@ -685,7 +715,7 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
   constexpr int kOwners = 32 - halo_lanes<C>();        // lanes with home cells
   const int wc = (warp - set * S.cell_warps) * kOwners * C;  // first cell of the warp
   const int r0 = wc + C * lane;                              // first of the lane's C home cells
-  float4* rec = (float4*)s.batch;  // [nt][2]: {c, fP, bin | imu << 20, G0}, {mu weights}
+  float4* rec = (float4*)s.batch;  // [nt][2]: {c, fP, imu, G0}, {mu weights}; set k uses [32 cell_warps k, ..)
 
   for (;;) {
     __syncthreads();
@@ -707,6 +737,7 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
       double lg = s_g.logg, ag;
       s_int[45] = (lg < X.g_min || lg > X.g_max) ? 1 : 0;
       s_int[44] = 0;
+      s_int[46] = tile.u0;  // next phase node of the deposit
       int ig = uhunt(lg, X.g_min, X.g_max, X.ng, ag);
       double wg[4];
       int ig0, ngt;
@@ -773,169 +804,211 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
     }
     __syncthreads();
 
-    // ---- deposit
+    // ---- deposit.  The tile's phase nodes u in [u0, u1) (u = bin * n_gl + GL
+    // point) go to the warp sets one at a time through a shared counter.  A set
+    // walks its node's elements jj = 0 .. n_act - 1 in order, 32 x cell_warps
+    // at a time: every thread evaluates one point (FP64), the visible points are
+    // compacted in order into the set's records, and every lane adds each record
+    // to its energies' FP32 partial sums; at the end of the node the sums are
+    // flushed with compensated FP64 atomics.  A node's sums thus depend on the
+    // tile's elements and the node only, not on the tile's node range, the sets
+    // or what else is in the batch.
     const DevGrid& G = p.grid;
     const int n_e = G.n_e;
-    // per home cell i of the lane: its energies, MAXE slots in pairs (fractions, partial sums)
-    int e0[C], cnt[C];
+    // per home cell i of the lane: MAXE energy slots in pairs (fractions, partial sums); the cells' energy
+    // ranges (cell_first) are read again at each flush, out of the record loop's registers
     f32x2 fE2[C][MAXE / 2], acc2[C][MAXE / 2];
 #pragma unroll
     for (int i = 0; i < C; ++i) {
       const int rc = r0 + i;
       const bool own = lane < kOwners && rc < G.span;
-      e0[i] = own ? G.cell_first[rc] : 0;
-      cnt[i] = own ? min(G.cell_first[rc + 1] - e0[i], MAXE) : 0;
+      const int e0 = own ? G.cell_first[rc] : 0;
+      const int cnt = own ? min(G.cell_first[rc + 1] - e0, MAXE) : 0;
 #pragma unroll
       for (int k = 0; k < MAXE / 2; ++k) {
-        fE2[i][k] = pk(2 * k < cnt[i] ? G.fEs[e0[i] + 2 * k] : 0.f, 2 * k + 1 < cnt[i] ? G.fEs[e0[i] + 2 * k + 1] : 0.f);
+        fE2[i][k] = pk(2 * k < cnt ? G.fEs[e0 + 2 * k] : 0.f, 2 * k + 1 < cnt ? G.fEs[e0 + 2 * k + 1] : 0.f);
         acc2[i][k] = pk(0.f, 0.f);
       }
     }
     const int mode = p.interp;
     const bool cubicE = mode != 4;
     const bool sg = mode == 1;
-    const double mu_min = s.mu[nmu - 1];
-    const int n_pp = p.n_gl > 0 ? p.n_bins * p.n_gl : p.n_bins;
-    const int n_pts = n_pp * n_act;
-    int cur_bin = -1;
-    double* flux_base = a.flux + p.flux_off;
-    const double out_scale = sp.out_scale;
+    const int ST = 32 * S.cell_warps;  // threads of a set
+    const int st = tid - set * ST;     // this thread's index in its set
+    float4* srec = rec + 2 * set * ST;  // the set's records
+    if (lane == 0) {
+      s_nvis[warp] = 0;
+      s_nclamp[warp] = 0;
+    }
 
-    auto flush = [&]() {
+    const double* den = s.mu + nmu;  // [nmu - 3][4] reciprocal Lagrange denominators
+    for (;;) {
+      // the set's next node: its index, bin, phase and weight, published in shared memory (kept out of the
+      // registers of the record loop below)
+      if (st == 0) {
+        const int u = atomicAdd(&s_int[46], 1);
+        s_node[set] = u;
+        if (u < tile.u1) {
+          int bin;
+          double ppt, wgl;
+          node_phase(p, u, bin, ppt, wgl);
+          s_bin[set] = bin;
+          s_ppt[set] = ppt;
+          s_wgl[set] = wgl;
+        }
+      }
+      set_sync(set, ST);
+      if (s_node[set] >= tile.u1) break;
+      for (int jb = 0; jb < n_act; jb += ST) {
+        // every thread evaluates one element at the node (FP64); the visible
+        // ones are compacted, in element order, into the set's records
+        bool vis = false, clamped = false;
+        float c = 0.f, fP = 0.f;
+        int G0 = 0, imu = 0;
+        float w4[4] = {0.f, 0.f, 0.f, 0.f};
+        const int jj = jb + st;
+        if (jj < n_act) {
+          double z = 0, mu = 0;
+          const double flux = node_point(p, s, rp, point, jj, s_ppt[set], z, mu);
+          if (flux != 0.0) {
+            vis = true;
+            if (mu < s.mu[nmu - 1]) mu = s.mu[nmu - 1];
+            c = (float)(flux * s_wgl[set]);
+            const double tP = (log10(z) - sp.l10kT - X.E_min) * X.inv_dE;
+            const double fl = floor(tP);
+            fP = (float)(tP - fl);
+            if (fP >= 1.f) fP = 0.99999994f;
+            G0 = G.iE_min + (int)fl;
+            clamped = (G.tE_lo + tP < 0.0) || (G.tE_hi + tP > (double)(nE - 1)) || sp.T_clamped || s_int[45];
+            // mu weights (cpu/nsx.hpp:173-321)
+            double am;
+            const int im = vhunt(s.mu, nmu, mu, am);
+            const bool linear_mu = (mode == 4) || ((mode == 2 || mode == 3) && im >= nmu - 5);
+            int start;
+            if (linear_mu) {
+              start = min(im, nmu - 4);
+              const int o = im - start;
 #pragma unroll
-      for (int i = 0; i < C; ++i)
+              for (int k = 0; k < 4; ++k) w4[k] = k == o ? (float)(1 - am) : (k == o + 1 ? (float)am : 0.f);
+            } else {
+              start = clampi(im - 1, 0, nmu - 4);
+              const double x0 = s.mu[start], x1 = s.mu[start + 1], x2 = s.mu[start + 2], x3 = s.mu[start + 3];
+              const double* rd = den + 4 * start;
+              w4[0] = (float)((mu - x1) * (mu - x2) * (mu - x3) * rd[0]);
+              w4[1] = (float)((mu - x0) * (mu - x2) * (mu - x3) * rd[1]);
+              w4[2] = (float)((mu - x0) * (mu - x1) * (mu - x3) * rd[2]);
+              w4[3] = (float)((mu - x0) * (mu - x1) * (mu - x2) * rd[3]);
+            }
+            imu = start;
+          }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, vis);
+        const unsigned bal_clamped = __ballot_sync(0xffffffffu, clamped);
+        if (lane == 0) {
+          s_nvis[warp] += __popc(bal);
+          s_nclamp[warp] += __popc(bal_clamped);
+        }
+        int nv, slot;
+        if (S.cell_warps == 1) {
+          nv = __popc(bal);
+          slot = __popc(bal & lanemask_lt());
+        } else {
+          const int w = st >> 5;
+          if (lane == 0) s_wcnt[warp] = __popc(bal);
+          set_sync(set, ST);
+          int before = 0;
+          nv = 0;
+          for (int k = 0; k < S.cell_warps; ++k) {
+            const int cw = s_wcnt[set * S.cell_warps + k];
+            before += k < w ? cw : 0;
+            nv += cw;
+          }
+          slot = before + __popc(bal & lanemask_lt());
+        }
+        if (vis) {
+          srec[2 * slot] = make_float4(c, fP, __int_as_float(imu), __int_as_float(G0));
+          srec[2 * slot + 1] = make_float4(w4[0], w4[1], w4[2], w4[3]);
+        }
+        set_sync(set, ST);
+        for (int b = 0; b < nv; ++b) {
+          const float4 rA = srec[2 * b], wA = srec[2 * b + 1];
+          const int g = __float_as_int(rA.w) + r0;  // first home cell of the lane for this point
+          float h[C + 4];
+          lane_window<C>(Sx, ldS, nE, g, __float_as_int(rA.z), wA, h);
+          float4 Q[C + 1];
+          if (cubicE) {
+            window_cubics<C>(h, Q);
+          } else {
+#pragma unroll
+            for (int i = 0; i <= C; ++i) Q[i] = make_float4(h[i + 1], h[i + 2] - h[i + 1], 0.f, 0.f);
+          }
+          // cells past an end hold the end value: H[0] is h[i] there; H[nE - 1]
+          // is h[i + 1], except where that window row is the extrapolated row nE
+          if (__any_sync(0xffffffffu, g < 0 || g + C > nE - 2)) {
+#pragma unroll
+            for (int i = 0; i <= C; ++i) {
+              const int gi = g + i;
+              if (gi < 0) Q[i] = make_float4(h[i], 0.f, 0.f, 0.f);
+              if (gi > nE - 2) Q[i] = make_float4(gi == nE ? h[i] : h[i + 1], 0.f, 0.f, 0.f);
+            }
+          }
+          const f32x2 cw2 = pk(rA.x, rA.x), fP2 = pk(rA.y, rA.y), m1 = pk(-1.f, -1.f);
+#pragma unroll
+          for (int i = 0; i < C; ++i) {
+            const f32x2 ax = pk(Q[i].x, Q[i].x), ay = pk(Q[i].y, Q[i].y), az = pk(Q[i].z, Q[i].z), aw = pk(Q[i].w, Q[i].w);
+            const f32x2 bx = pk(Q[i + 1].x, Q[i + 1].x), by = pk(Q[i + 1].y, Q[i + 1].y), bz = pk(Q[i + 1].z, Q[i + 1].z),
+                        bw = pk(Q[i + 1].w, Q[i + 1].w);
+#pragma unroll
+            for (int k = 0; k < MAXE / 2; ++k) {
+              // split coordinate t = fE + fP: cell i below 1, cell i + 1 at t - 1
+              // above; both cubics are evaluated and the result selected
+              const f32x2 t0 = add2(fE2[i][k], fP2), t1 = add2(t0, m1);
+              const f32x2 v0 = fma2(fma2(fma2(aw, t0, az), t0, ay), t0, ax);
+              const f32x2 v1 = fma2(fma2(fma2(bw, t1, bz), t1, by), t1, bx);
+              float ta, tb, a0, b0, a1, b1;
+              upk(t0, ta, tb);
+              upk(v0, a0, b0);
+              upk(v1, a1, b1);
+              float va = ta >= 1.f ? a1 : a0, vb = tb >= 1.f ? b1 : b0;
+              if (sg) {
+                va = fmaxf(va, 0.f);
+                vb = fmaxf(vb, 0.f);
+              }
+              acc2[i][k] = fma2(cw2, pk(va, vb), acc2[i][k]);
+            }
+          }
+        }
+        set_sync(set, ST);  // the records are rewritten by the next step
+      }
+      // the node's partial sums into the flux pool
+      const int bin = s_bin[set];
+      double* flux_base = a.flux + p.flux_off;
+      double* comp_base = a.comp ? a.comp + p.flux_off : nullptr;
+      const double out_scale = sp.out_scale;
+#pragma unroll
+      for (int i = 0; i < C; ++i) {
+        const int rc = r0 + i;
+        const bool own = lane < kOwners && rc < G.span;
+        const int e0 = own ? G.cell_first[rc] : 0;
+        const int cnt = own ? min(G.cell_first[rc + 1] - e0, MAXE) : 0;
 #pragma unroll
         for (int k = 0; k < MAXE; ++k) {
           float lo, hi;
           upk(acc2[i][k / 2], lo, hi);
           const float v = (k & 1) ? hi : lo;
-          if (k < cnt[i] && v != 0.f) {
-            const int e = G.perm[e0[i] + k];
-            atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)v * out_scale * G.invE[e]);
+          if (k < cnt && v != 0.f) {
+            const int e = G.perm[e0 + k];
+            const size_t o = (size_t)bin * n_e + e;
+            comp_add(flux_base + o, comp_base ? comp_base + o : nullptr, (double)v * out_scale * G.invE[e]);
           }
           if (k & 1) acc2[i][k / 2] = pk(0.f, 0.f);
         }
-    };
-
-    const double* den = s.mu + nmu;  // [nmu - 3][4] reciprocal Lagrange denominators
-    for (int q0 = 0; q0 < n_pts; q0 += nt) {
-      // every thread evaluates one phase point (FP64); visible ones are
-      // compacted, in order, into the point records
-      bool vis = false, clamped = false;
-      float c = 0.f, fP = 0.f;
-      int G0 = 0, bin = 0, imu = 0;
-      float w4[4] = {0.f, 0.f, 0.f, 0.f};
-      const int q = q0 + tid;
-      if (q < n_pts) {
-        double wgl, z = 0, mu = 0;
-        const double flux = phase_point(p, s, rp, point, n_act, q, bin, wgl, z, mu);
-        if (flux != 0.0) {
-          vis = true;
-          if (mu < mu_min) mu = mu_min;
-          c = (float)(flux * wgl);
-          const double tP = (log10(z) - sp.l10kT - X.E_min) * X.inv_dE;
-          const double fl = floor(tP);
-          fP = (float)(tP - fl);
-          if (fP >= 1.f) fP = 0.99999994f;
-          G0 = G.iE_min + (int)fl;
-          clamped = (G.tE_lo + tP < 0.0) || (G.tE_hi + tP > (double)(nE - 1)) || sp.T_clamped || s_int[45];
-          // mu weights (cpu/nsx.hpp:173-321)
-          double am;
-          const int im = vhunt(s.mu, nmu, mu, am);
-          const bool linear_mu = (mode == 4) || ((mode == 2 || mode == 3) && im >= nmu - 5);
-          int start;
-          if (linear_mu) {
-            start = min(im, nmu - 4);
-            const int o = im - start;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) w4[k] = k == o ? (float)(1 - am) : (k == o + 1 ? (float)am : 0.f);
-          } else {
-            start = clampi(im - 1, 0, nmu - 4);
-            const double x0 = s.mu[start], x1 = s.mu[start + 1], x2 = s.mu[start + 2], x3 = s.mu[start + 3];
-            const double* rd = den + 4 * start;
-            w4[0] = (float)((mu - x1) * (mu - x2) * (mu - x3) * rd[0]);
-            w4[1] = (float)((mu - x0) * (mu - x2) * (mu - x3) * rd[1]);
-            w4[2] = (float)((mu - x0) * (mu - x1) * (mu - x3) * rd[2]);
-            w4[3] = (float)((mu - x0) * (mu - x1) * (mu - x2) * rd[3]);
-          }
-          imu = start;
-        }
       }
-      int nv;
-      const int slot = block_compact(vis, s_int, &nv);
-      if (vis) {
-        rec[2 * slot] = make_float4(c, fP, __uint_as_float((unsigned)bin | ((unsigned)imu << 20)), __int_as_float(G0));
-        rec[2 * slot + 1] = make_float4(w4[0], w4[1], w4[2], w4[3]);
-        if (clamped) atomicAdd(&s_int[44], 1);
-      }
-      __syncthreads();
-      if (tid == 0) {
-        if (nv) atomicAdd(&p.stats[3], (unsigned long long)nv);
-        if (s_int[44]) atomicAdd(&p.stats[4], (unsigned long long)s_int[44]);
-        s_int[44] = 0;
-      }
-
-      // each warp set takes a contiguous run of the records (one flush per bin
-      // change in its run)
-      const int b_end = (int)((long long)nv * (set + 1) / n_sets);
-      for (int b = (int)((long long)nv * set / n_sets); b < b_end; ++b) {
-        const float4 rA = rec[2 * b], wA = rec[2 * b + 1];
-        const unsigned packed = __float_as_uint(rA.z);
-        const int bin = (int)(packed & 0xFFFFFu);
-        if (bin != cur_bin) {
-          if (cur_bin >= 0) flush();
-          cur_bin = bin;
-        }
-        const int g = __float_as_int(rA.w) + r0;  // first home cell of the lane for this point
-        float h[C + 4];
-        lane_window<C>(Sx, ldS, nE, g, (int)(packed >> 20), wA, h);
-        float4 Q[C + 1];
-        if (cubicE) {
-          window_cubics<C>(h, Q);
-        } else {
-#pragma unroll
-          for (int i = 0; i <= C; ++i) Q[i] = make_float4(h[i + 1], h[i + 2] - h[i + 1], 0.f, 0.f);
-        }
-        // cells past an end hold the end value: H[0] is h[i] there; H[nE - 1]
-        // is h[i + 1], except where that window row is the extrapolated row nE
-        if (__any_sync(0xffffffffu, g < 0 || g + C > nE - 2)) {
-#pragma unroll
-          for (int i = 0; i <= C; ++i) {
-            const int gi = g + i;
-            if (gi < 0) Q[i] = make_float4(h[i], 0.f, 0.f, 0.f);
-            if (gi > nE - 2) Q[i] = make_float4(gi == nE ? h[i] : h[i + 1], 0.f, 0.f, 0.f);
-          }
-        }
-        const f32x2 cw2 = pk(rA.x, rA.x), fP2 = pk(rA.y, rA.y), m1 = pk(-1.f, -1.f);
-#pragma unroll
-        for (int i = 0; i < C; ++i) {
-          const f32x2 ax = pk(Q[i].x, Q[i].x), ay = pk(Q[i].y, Q[i].y), az = pk(Q[i].z, Q[i].z), aw = pk(Q[i].w, Q[i].w);
-          const f32x2 bx = pk(Q[i + 1].x, Q[i + 1].x), by = pk(Q[i + 1].y, Q[i + 1].y), bz = pk(Q[i + 1].z, Q[i + 1].z),
-                      bw = pk(Q[i + 1].w, Q[i + 1].w);
-#pragma unroll
-          for (int k = 0; k < MAXE / 2; ++k) {
-            // split coordinate t = fE + fP: cell i below 1, cell i + 1 at t - 1
-            // above; both cubics are evaluated and the result selected
-            const f32x2 t0 = add2(fE2[i][k], fP2), t1 = add2(t0, m1);
-            const f32x2 v0 = fma2(fma2(fma2(aw, t0, az), t0, ay), t0, ax);
-            const f32x2 v1 = fma2(fma2(fma2(bw, t1, bz), t1, by), t1, bx);
-            float ta, tb, a0, b0, a1, b1;
-            upk(t0, ta, tb);
-            upk(v0, a0, b0);
-            upk(v1, a1, b1);
-            float va = ta >= 1.f ? a1 : a0, vb = tb >= 1.f ? b1 : b0;
-            if (sg) {
-              va = fmaxf(va, 0.f);
-              vb = fmaxf(vb, 0.f);
-            }
-            acc2[i][k] = fma2(cw2, pk(va, vb), acc2[i][k]);
-          }
-        }
-      }
-      // no barrier here: the next round writes records only after the barriers
-      // of its compaction, which every warp reaches after this loop
     }
-    if (cur_bin >= 0) flush();
+    if (lane == 0) {
+      if (s_nvis[warp]) atomicAdd(&p.stats[3], (unsigned long long)s_nvis[warp]);
+      if (s_nclamp[warp]) atomicAdd(&p.stats[4], (unsigned long long)s_nclamp[warp]);
+    }
   }
 }
 
@@ -969,7 +1042,10 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
 
     const DevGrid& G = p.grid;
     const int n_e = G.n_e;
-    Real E[NE_T], acc[NE_T];
+    // partial sums in FP64 in every arithmetic (the FP32 integrand's values are summed exactly enough that the
+    // grouping of the points does not show)
+    Real E[NE_T];
+    double acc[NE_T];
 #pragma unroll
     for (int k = 0; k < NE_T; ++k) {
       const int e = tid + k * nt;
@@ -977,17 +1053,20 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
       acc[k] = 0;
     }
     const Real kT = (Real)sp.kT;
-    const int n_pp = p.n_gl > 0 ? p.n_bins * p.n_gl : p.n_bins;
+    const int n_pp = tile.u1 - tile.u0;  // the tile's phase nodes
     const int n_pts = n_pp * n_act;
     int cur_bin = -1;
     double* flux_base = a.flux + p.flux_off;
+    double* comp_base = a.comp ? a.comp + p.flux_off : nullptr;
     const double out_scale = sp.out_scale;
     auto flush = [&]() {
 #pragma unroll
       for (int k = 0; k < NE_T; ++k) {
         const int e = tid + k * nt;
-        if (e < n_e && acc[k] != (Real)0)
-          atomicAdd(flux_base + (size_t)cur_bin * n_e + e, (double)acc[k] * out_scale * G.invE[e]);
+        if (e < n_e && acc[k] != 0.0) {
+          const size_t o = (size_t)cur_bin * n_e + e;
+          comp_add(flux_base + o, comp_base ? comp_base + o : nullptr, acc[k] * out_scale * G.invE[e]);
+        }
         acc[k] = 0;
       }
     };
@@ -1037,7 +1116,7 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
         const double scale = out_scale;
         unsigned int n_vis = 0;
         for (int it = tid; it < n_items; it += nt) {
-          const int k = it % n_pp, seg = it / n_pp;
+          const int k = tile.u0 + it % n_pp, seg = it / n_pp;
           const int jj0 = (int)((long long)n_act * seg / segs), jj1 = (int)((long long)n_act * (seg + 1) / segs);
           int bin, g = 0;
           if (n_gl > 0) {
@@ -1081,7 +1160,10 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
           }
 #pragma unroll
           for (int e = 0; e < kPhaseMajorMaxE; ++e)
-            if (e < n_e && acc[e] != 0.0) atomicAdd(flux_base + (size_t)bin * n_e + e, acc[e] * scale * invE_s[e]);
+            if (e < n_e && acc[e] != 0.0) {
+              const size_t o = (size_t)bin * n_e + e;
+              comp_add(flux_base + o, comp_base ? comp_base + o : nullptr, acc[e] * scale * invE_s[e]);
+            }
         }
         const int lane = tid & 31;
 #pragma unroll
@@ -1112,7 +1194,8 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
           if (pp0 + k < pp1) {
             double wgl, z = 0;
             const double flux =
-                phase_point_at(s, n_fp, P0, inv_dp_use, n_gl, inv_bins, phase_shift, pp0 + k, mono, hint, bin, wgl, z);
+                phase_point_at(s, n_fp, P0, inv_dp_use, n_gl, inv_bins, phase_shift, tile.u0 + pp0 + k, mono, hint, bin,
+                               wgl, z);
             if (flux != 0.0) {
               vis = true;
               c = flux * wgl;
@@ -1128,19 +1211,22 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
           const bool head = (lane == 0 || prev_bin != bin) && bin != INT_MAX;
           const Real cb = (Real)c, zb = (Real)zz;
           for (int e = 0; e < n_e; ++e) {
-            Real v = 0;
+            double v = 0;
             if (vis) {
               const Real Ee = (staged ? E_s[e] : (Real)G.E[e]) * zb;
-              v = cb * (Ee * Ee * Ee / expm1(Ee * inv_kT));  // Ibb without its constant (in out_scale)
+              v = (double)(cb * (Ee * Ee * Ee / expm1(Ee * inv_kT)));  // Ibb without its constant (in out_scale)
             }
 #pragma unroll
             for (int off = 1; off < 32; off <<= 1) {
-              const Real o = __shfl_down_sync(0xffffffffu, v, off);
+              const double o = __shfl_down_sync(0xffffffffu, v, off);
               const int ob = __shfl_down_sync(0xffffffffu, bin, off);
               if (lane + off < 32 && ob == bin) v += o;
             }
-            if (head && v != (Real)0)
-              atomicAdd(flux_base + (size_t)bin * n_e + e, (double)v * scale * (staged ? invE_s[e] : G.invE[e]));
+            if (head && v != 0.0) {
+              const size_t o = (size_t)bin * n_e + e;
+              comp_add(flux_base + o, comp_base ? comp_base + o : nullptr,
+                       v * scale * (staged ? invE_s[e] : G.invE[e]));
+            }
           }
         }
       }
@@ -1156,7 +1242,7 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
       const int q = q0 + tid;
       if (q < n_pts) {
         double wgl, z = 0, mu = 0;
-        const double flux = phase_point(p, s, rp, point, n_act, q, bin, wgl, z, mu);
+        const double flux = phase_point(p, s, rp, point, n_act, tile.u0, q, bin, wgl, z, mu);
         if (flux != 0.0) {
           vis = true;
           c = flux * wgl;
@@ -1184,7 +1270,7 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
           // Ibb(E, kT) = Ibb_constant E^3 / expm1(E / kT) (cpu/unit.hpp:28-31); the constant is in out_scale
           const Real Ee = E[k] * zb;
           const Real I = Ee * Ee * Ee / expm1(Ee / kT);
-          acc[k] += cb * I;
+          acc[k] += (double)(cb * I);
         }
       }
       __syncthreads();
@@ -1263,9 +1349,11 @@ __device__ __forceinline__ void push_tile(const WorkQueue& q, const Tile& t) {
 }
 
 // One CTA per (profile, spot, ring block): a spot's rings are shared by
-// ring_blocks CTAs, so that a small batch plans on many SMs at once.
+// ring_blocks CTAs, so that a small batch plans on many SMs at once.  Every
+// chunk of a ring's candidate range becomes ceil(nodes / nodes_per_tile) tiles,
+// one per range of phase nodes.
 __global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const DevLens L, const WorkQueue q, int chunk,
-                            int ring_blocks) {
+                            int nodes_per_tile, int ring_blocks) {
   const int ps = blockIdx.x / ring_blocks, rb = blockIdx.x - ps * ring_blocks;
   const int pi = ps / kMaxSpots, si = ps % kMaxSpots;
   if (pi >= n_profiles) return;
@@ -1273,6 +1361,15 @@ __global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const De
   if (si >= p.n_spots) return;
   const DevSpot& sp = p.spot[si];
   const bool nsx = p.atmosphere == 0;
+  const int n_nodes = p.n_bins * max(p.n_gl, 1);
+  const int npt = nodes_per_tile > 0 ? min(nodes_per_tile, n_nodes) : n_nodes;
+  auto push_nodes = [&](Tile t) {
+    for (int u = 0; u < n_nodes; u += npt) {
+      t.u0 = (short)u;
+      t.u1 = (short)min(u + npt, n_nodes);
+      push_tile(q, t);
+    }
+  };
   if (sp.kind == 1) {
     if (sp.i_lo > sp.i_hi || rb != 0) return;  // outside the batch's ring window, or another block's
     if (threadIdx.x == 0) {
@@ -1283,7 +1380,7 @@ __global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const De
         atomicAdd(&p.stats[2], 1ull);
         atomicAdd(&p.stats[5], 1ull);
       } else {
-        push_tile(q, Tile{pi, (short)si, 1, 0, 0, 1});
+        push_nodes(Tile{pi, (short)si, 1, 0, 0, 1, 0, 0});
       }
     }
     return;
@@ -1314,7 +1411,7 @@ __global__ void plan_kernel(const DevProfile* profiles, int n_profiles, const De
     for (int k = 0; k < nr; ++k)
       for (int j0 = r[k][0]; j0 <= r[k][1]; j0 += chunk) {
         const int j1 = min(j0 + chunk, r[k][1] + 1);
-        push_tile(q, Tile{pi, (short)si, (short)(first ? 1 : 0), i, j0, j1});
+        push_nodes(Tile{pi, (short)si, (short)(first ? 1 : 0), i, j0, j1, 0, 0});
         first = false;
       }
   }
@@ -1514,11 +1611,27 @@ int max_active_ctas(const IntegrandShape& s) {
 }
 
 cudaError_t launch_plan(const DevProfile* profiles, int n_profiles, const DevLens& lens, const WorkQueue& q, int chunk,
-                        cudaStream_t st) {
+                        int nodes_per_tile, cudaStream_t st) {
   if (n_profiles <= 0) return cudaSuccess;
   // a few profiles: up to 32 CTAs share each spot's rings (4N - 1 of them at most)
   const int ring_blocks = std::max(1, std::min(32, 64 / n_profiles));
-  plan_kernel<<<n_profiles * kMaxSpots * ring_blocks, 128, 0, st>>>(profiles, n_profiles, lens, q, chunk, ring_blocks);
+  plan_kernel<<<n_profiles * kMaxSpots * ring_blocks, 128, 0, st>>>(profiles, n_profiles, lens, q, chunk,
+                                                                      nodes_per_tile, ring_blocks);
+  return cudaGetLastError();
+}
+
+namespace {
+// flux += comp: the compensation pool's rounding errors back into the flux pool before the fold
+__global__ void add_comp_kernel(double* __restrict__ flux, const double* __restrict__ comp, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    flux[i] += comp[i];
+}
+}  // namespace
+
+cudaError_t launch_add_comp(double* flux, const double* comp, long long n, int sm_count, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((n + 255) / 256, (long long)sm_count * 8);
+  add_comp_kernel<<<(unsigned)blocks, 256, 0, st>>>(flux, comp, n);
   return cudaGetLastError();
 }
 

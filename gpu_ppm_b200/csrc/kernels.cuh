@@ -40,11 +40,15 @@ struct KernelArgs {
   DevNsx nsx;
   WorkQueue queue;
   double* flux;  // pool
+  double* comp;  // compensation pool of the flux pool's atomic additions (nullptr: plain additions)
   IntegrandShape shape;
 };
 
+// chunk: candidate elements per tile; nodes_per_tile: phase nodes per tile (<= 0: all of a profile's)
 cudaError_t launch_plan(const DevProfile* profiles, int n_profiles, const DevLens& lens, const WorkQueue& q, int chunk,
-                        cudaStream_t st);
+                        int nodes_per_tile, cudaStream_t st);
+// flux[i] += comp[i], i < n
+cudaError_t launch_add_comp(double* flux, const double* comp, long long n, int sm_count, cudaStream_t st);
 cudaError_t launch_integrand(const KernelArgs& a, int grid, cudaStream_t st);
 // counts[c][b] = alpha * sum_E rsp[c][E] * flux[b][E] for each listed profile, FP64 or FP32 SIMT
 struct FoldJob {

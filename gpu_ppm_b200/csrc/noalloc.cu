@@ -131,6 +131,9 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   off += up256(sizeof(float) * (size_t)n_e);
   const size_t o_cf = off;
   off += up256(sizeof(int) * n_cf);
+  const int ring_words = 4 * N / 32 + 1;
+  const size_t o_rseen = off;
+  off += up256(sizeof(unsigned) * kMaxSpots * (size_t)ring_words);
   const size_t o_tiles = off;
   if (off > kScratchBytes)
     throw Error(PPM_E_RANGE, "ppm_profile_noalloc: N_side " + std::to_string(N) + " / n_fine " + std::to_string(nf) +
@@ -168,17 +171,17 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   DevProfile d;
   unsigned long long* stats = (unsigned long long*)(base + o_stats);
   fill_profile(p, d, 0, stats, (const double*)(base + o_ring), (const double*)(base + o_fine), g, ring_rows);
-  // work-queue bound (as in batch_build, with its tile size)
-  const long long pts = (long long)p.n_bins * std::max(1, p.n_gl);
-  const int chunk = tile_chunk(spot_elements(p) * (double)pts, pts);
-  long long cap = 0;
-  for (int s = 0; s < p.n_spots; ++s) {
-    const DevSpot& sp = d.spot[s];
-    if (sp.kind == PPM_SPOT_POINT)
-      cap += 1;
-    else if (sp.i_hi >= sp.i_lo)
-      cap += (long long)(sp.i_hi - sp.i_lo + 1) * (2 + (4ll * N + chunk - 1) / chunk);
-  }
+  d.ring_seen = (unsigned*)(base + o_rseen);
+  d.ring_words = ring_words;
+  // kernel and tiling as batch_build gives a one-profile batch
+  const bool bb64 = !nsx_atm && p.precision == PPM_PREC_FP64;
+  IntegrandShape shape = choose_shape(nsx_atm, bb64, n_e, nf, g.span + 1, g.maxe, p.n_bins);
+  const bool pooled = nsx_atm && !shape.cellk;
+  GroupWork w;
+  w.add(p, d);
+  int chunk = 0, npt = 0;
+  group_tiling(pooled, w, 0, &chunk, &npt);
+  const long long cap = tile_bound(p, d, chunk, npt);
   if (cap > tile_cap)
     throw Error(PPM_E_RANGE, "ppm_profile_noalloc: the profile needs up to " + std::to_string(cap) +
                                  " work tiles, the 1 MiB scratch array holds " + std::to_string(tile_cap) +
@@ -207,6 +210,7 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   ck(cudaMemsetAsync(base + o_stats, 0, sizeof(unsigned long long) * kStats, st), "counter clear");
   ck(cudaMemsetAsync(base + o_ctrl, 0, sizeof(int) * 16, st), "queue clear");
   ck(cudaMemsetAsync(base + o_status, 0, sizeof(int) * 4, st), "status clear");
+  ck(cudaMemsetAsync(base + o_rseen, 0, sizeof(unsigned) * kMaxSpots * (size_t)ring_words, st), "ring bits clear");
 
   int* ctrl = (int*)(base + o_ctrl);
   KernelArgs a{};
@@ -214,18 +218,18 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   a.lens = lens;
   a.nsx = nsx;
   a.flux = flux_d;
+  a.comp = nullptr;  // no room for a compensation pool: plain atomic additions
   WorkQueue& q = a.queue;
   q.tiles = (Tile*)(base + o_tiles);
   q.capacity = (int)cap;
   q.n_tiles = ctrl;
   q.next = ctrl + 1;
   q.overflow = ctrl + 2;
-  const bool bb64 = !nsx_atm && p.precision == PPM_PREC_FP64;
-  a.shape = choose_shape(nsx_atm, bb64, n_e, nf, g.span + 1, g.maxe, p.n_bins);
+  a.shape = shape;
   ck(configure_integrand_smem(a.shape), "shared-memory attribute");
   const int occ = max_active_ctas(a.shape);
   if (occ < 1) throw Error(PPM_E_RANGE, "ppm_profile_noalloc: launch shape does not fit on an SM");
-  ck(launch_plan(a.profiles, 1, lens, q, chunk, st), "plan launch");
+  ck(launch_plan(a.profiles, 1, lens, q, chunk, npt, st), "plan launch");
   ck(launch_integrand(a, (int)std::min<long long>((long long)sm_count * occ, std::max(1ll, cap)), st),
      "integrand launch");
   if (counts_d) {

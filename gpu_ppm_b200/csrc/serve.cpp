@@ -203,7 +203,7 @@ struct Server {
   // Copies one finished batch's results into the callers' buffers (no lock held).
   static std::vector<std::pair<uint64_t, Done>> copy_out(const InFlight& f) {
     std::vector<std::pair<uint64_t, Done>> out(f.reqs.size());
-    const bool overflow = f.ctrl[2] || f.ctrl[5] || f.ctrl[8];
+    const bool overflow = f.ctrl[2] || f.ctrl[5] || f.ctrl[8] || f.ctrl[11];
     for (size_t i = 0; i < f.reqs.size(); ++i) {
       const Request& r = f.reqs[i];
       Done& d = out[i].second;
@@ -379,13 +379,20 @@ struct Server {
 
 size_t Engine::request_bytes(const ppm_params& p) const {
   const size_t n_e = grids[p.energy_grid].E.size();
-  size_t b = sizeof(double) * (size_t)p.n_bins * n_e;
+  size_t b = 2 * sizeof(double) * (size_t)p.n_bins * n_e;  // flux and its compensation pool
   if (p.response >= 0) b += sizeof(double) * (size_t)resps[p.response].n_ch * p.n_bins;
+  // work tiles: the larger of the finest element chunks (pooled kernel) and the tuned chunks with the most
+  // phase-node splits (home-cell and blackbody kernels)
+  const size_t nodes = (size_t)p.n_bins * std::max(1, p.n_gl);
+  const size_t splits = std::max<size_t>(1, nodes / kMinNodesPerTile);
   for (int s = 0; s < p.n_spots; ++s) {
     const long long rings = p.spots[s].kind == PPM_SPOT_POINT ? 1 : 4ll * p.n_side - 1;
-    const size_t chunk = (size_t)std::min(tune.chunk, tune.small_chunk);  // the finest tiles a batch may use
-    b += sizeof(Tile) * (size_t)rings * (2 + (4 * (size_t)p.n_side + chunk - 1) / chunk);
+    const size_t fine = (size_t)std::min(tune.chunk, tune.small_chunk);
+    const size_t by_elements = (size_t)rings * (2 + (4 * (size_t)p.n_side + fine - 1) / fine);
+    const size_t by_nodes = (size_t)rings * (2 + (4 * (size_t)p.n_side + tune.chunk - 1) / tune.chunk) * splits;
+    b += sizeof(Tile) * std::max(by_elements, by_nodes);
   }
+  b += sizeof(unsigned) * kMaxSpots * (4 * (size_t)p.n_side / 32 + 1);  // ring bits
   return b + sizeof(DevProfile) + sizeof(unsigned long long) * kStats + 4096;
 }
 

@@ -52,9 +52,9 @@ def setup():
 
 
 def check_info(info, golden):
-    """Active elements, integrated phase points and dropped rings equal the oracle's."""
+    """Active elements, integrated phase points, dropped rings and rings with active elements equal the oracle's."""
     want = dict(zip(mcg.INFO_FIELDS, (int(x) for x in golden)))
-    for k in ("n_active", "n_points", "n_dropped_rings"):
+    for k in ("n_active", "n_points", "n_dropped_rings", "n_rings"):
         assert getattr(info, k) == want[k], (k, getattr(info, k), want[k])
 
 
