@@ -159,7 +159,7 @@ Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   PPM_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, cfg.device));
   PPM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   // launch-shape overrides for experiments: PPM_PB, PPM_CHUNK, PPM_SMALL_CHUNK, PPM_NE_T, PPM_MINB, PPM_KERNEL,
-  // PPM_SETS, PPM_CPL
+  // PPM_SETS, PPM_CPL, PPM_SPLITS
   if (const char* v = std::getenv("PPM_PB")) tune.pb = std::max(1, std::atoi(v));
   if (const char* v = std::getenv("PPM_CHUNK")) tune.chunk = std::max(32, std::atoi(v));
   if (const char* v = std::getenv("PPM_SMALL_CHUNK")) tune.small_chunk = std::max(32, std::atoi(v));
@@ -168,6 +168,7 @@ Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   if (const char* v = std::getenv("PPM_KERNEL")) tune.kernel = std::atoi(v) ? 1 : 0;
   if (const char* v = std::getenv("PPM_SETS")) tune.sets = std::max(0, std::atoi(v));
   if (const char* v = std::getenv("PPM_CPL")) tune.cpl = std::max(0, std::min(3, std::atoi(v)));
+  if (const char* v = std::getenv("PPM_SPLITS")) tune.splits = std::max(0, std::atoi(v));
   for (int k = 0; k < 4; ++k) PPM_CUDA(cudaEventCreate(&ev[k]));
   PPM_CUDA(cudaMalloc(&d_err, sizeof(int)));
   PPM_CUDA(cudaMemset(d_err, 0, sizeof(int)));
@@ -950,6 +951,8 @@ void GroupWork::add(const ppm_params& p, const DevProfile& d) {
   const long long pts = (long long)p.n_bins * std::max(1, p.n_gl);
   pts_max = std::max(pts_max, pts);
   nodes_max = std::max(nodes_max, (int)pts);
+  ne_max = std::max(ne_max, d.n_e);
+  elements += Engine::spot_elements(p);
   work += Engine::spot_elements(p) * (double)pts;
   for (int s = 0; s < p.n_spots; ++s) {
     const DevSpot& sp = d.spot[s];
@@ -963,9 +966,11 @@ void GroupWork::add(const ppm_params& p, const DevProfile& d) {
 // Tiling of one kernel group.  The home-cell NSX and the blackbody kernels
 // keep the tuned element chunk in every batch, so that a profile's tiles cover
 // the same elements alone and in any batch; a batch with few rings is spread
-// over the SMs by splitting each tile's phase nodes instead (about 8 tiles per
-// CTA slot, at least kMinNodesPerTile nodes per tile).  The pooled kernel
-// splits the elements (tile_chunk) and takes all nodes.
+// over the SMs by splitting each tile's phase nodes instead: about 8 tiles per
+// CTA slot, but every tile keeps at least kMinNodesPerTile nodes and enough
+// (element, node, energy) evaluations to outweigh its prologue (the FP64
+// fine-phase sweep and the tables it stages, repeated by every tile of a ring).
+// The pooled kernel splits the elements (tile_chunk) and takes all nodes.
 void Engine::group_tiling(bool pooled, const GroupWork& w, int chunk_override, int* chunk, int* npt) const {
   if (pooled) {
     *chunk = chunk_override > 0 ? chunk_override : tile_chunk(w.work, w.pts_max);
@@ -973,10 +978,15 @@ void Engine::group_tiling(bool pooled, const GroupWork& w, int chunk_override, i
     return;
   }
   *chunk = chunk_override > 0 ? chunk_override : tune.chunk;
+  const double rings = std::max<double>(1.0, (double)w.rings);
   const double want = 8.0 * sm_count * 3;
-  const double splits_d = std::ceil(want / std::max<double>(1.0, (double)w.rings));
-  const int max_splits = std::max(1, w.nodes_max / kMinNodesPerTile);
-  const int splits = (int)std::max(1.0, std::min<double>(splits_d, max_splits));
+  double splits_d = std::ceil(want / rings);
+  // nodes per tile for kMinEvalsPerTile evaluations at the group's mean active elements per ring
+  const double per_ring = std::max(1.0, std::min<double>(w.elements / rings, *chunk));
+  const double min_nodes = std::max<double>(kMinNodesPerTile, std::ceil(kMinEvalsPerTile / (per_ring * w.ne_max)));
+  splits_d = std::min(splits_d, std::floor(w.nodes_max / min_nodes));
+  int splits = (int)std::max(1.0, splits_d);
+  if (tune.splits > 0) splits = std::min(tune.splits, std::max(1, w.nodes_max));
   *npt = splits <= 1 ? 0 : (w.nodes_max + splits - 1) / splits;
 }
 

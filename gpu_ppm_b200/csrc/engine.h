@@ -179,11 +179,14 @@ void split_grid(const std::vector<double>& E, double inv_dE, GridSplit& out);
 
 // Work estimate of one kernel group of a batch (the tiling's inputs).
 constexpr int kMinNodesPerTile = 8;
+constexpr double kMinEvalsPerTile = 65536;  // (element, node, energy) evaluations per tile, at least
 struct GroupWork {
   double work = 0;        // phase points, estimated from the spots' areas
   long long pts_max = 1;  // phase points per element, largest profile
   long long rings = 0;    // rings that may hold active elements
+  double elements = 0;    // active elements, estimated from the spots' areas
   int nodes_max = 1;      // phase nodes per profile, largest profile
+  int ne_max = 1;         // energies per profile, largest grid
   void add(const ppm_params& p, const DevProfile& d);
 };
 
@@ -196,6 +199,7 @@ struct Tuning {
   int kernel = 0;    // NSX integrand: 0 = home-cell kernel where the grid allows, 1 = pooled-polynomial kernel
   int sets = 0;      // home-cell kernel: warp sets per CTA (0 = about 256 threads)
   int cpl = 0;       // home-cell kernel: cells per lane (0 = by estimated cost)
+  int splits = 0;    // phase-node splits per element chunk (0 = by the batch's work)
 };
 
 // Observed counts [n_ch][n_bins] for fit statistics.
