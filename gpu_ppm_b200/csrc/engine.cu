@@ -159,7 +159,7 @@ Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   PPM_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, cfg.device));
   PPM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   // launch-shape overrides for experiments: PPM_PB, PPM_CHUNK, PPM_SMALL_CHUNK, PPM_NE_T, PPM_MINB, PPM_KERNEL,
-  // PPM_SETS, PPM_CPL, PPM_SPLITS
+  // PPM_SETS, PPM_CPL, PPM_SPLITS, PPM_BB_NT
   if (const char* v = std::getenv("PPM_PB")) tune.pb = std::max(1, std::atoi(v));
   if (const char* v = std::getenv("PPM_CHUNK")) tune.chunk = std::max(32, std::atoi(v));
   if (const char* v = std::getenv("PPM_SMALL_CHUNK")) tune.small_chunk = std::max(32, std::atoi(v));
@@ -169,6 +169,7 @@ Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   if (const char* v = std::getenv("PPM_SETS")) tune.sets = std::max(0, std::atoi(v));
   if (const char* v = std::getenv("PPM_CPL")) tune.cpl = std::max(0, std::min(3, std::atoi(v)));
   if (const char* v = std::getenv("PPM_SPLITS")) tune.splits = std::max(0, std::atoi(v));
+  if (const char* v = std::getenv("PPM_BB_NT")) tune.bb_nt = std::atoi(v) >= 512 ? 512 : (std::atoi(v) > 0 ? 256 : 0);
   for (int k = 0; k < 4; ++k) PPM_CUDA(cudaEventCreate(&ev[k]));
   PPM_CUDA(cudaMalloc(&d_err, sizeof(int)));
   PPM_CUDA(cudaMemset(d_err, 0, sizeof(int)));
@@ -674,12 +675,18 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
   for (int v = 0; v < NV; ++v)
     for (int i = 0; i < n; ++i)
       if (vof[i] == v) order.push_back(i);
-  B.d_stats = (unsigned long long*)B.mem.alloc(sizeof(unsigned long long) * kStats * (size_t)n);
   // ring bits per profile and spot (rings 0 .. 4 N_side - 1)
   std::vector<long long> ring_off(n + 1, 0);
   for (int i = 0; i < n; ++i) ring_off[i + 1] = ring_off[i] + (long long)kMaxSpots * (4ll * ps[i].n_side / 32 + 1);
   B.ring_words = ring_off[n];
-  B.d_ring_seen = (unsigned*)B.mem.alloc(sizeof(unsigned) * (size_t)B.ring_words);
+  // the counters, the ring bits and the queue control words in one block (cleared by one memset per pass)
+  const size_t stats_bytes = sizeof(unsigned long long) * kStats * (size_t)n;
+  const size_t ring_bytes = (sizeof(unsigned) * (size_t)B.ring_words + 63) / 64 * 64;
+  B.small_bytes = stats_bytes + ring_bytes + sizeof(int) * 16;
+  unsigned char* small = (unsigned char*)B.mem.alloc(B.small_bytes);
+  B.d_stats = (unsigned long long*)small;
+  B.d_ring_seen = (unsigned*)(small + stats_bytes);
+  B.d_ctrl = (int*)(small + stats_bytes + ring_bytes);
   std::vector<DevProfile> hp(n);
   GroupWork gw[NV];
   for (int k = 0; k < n; ++k) {
@@ -717,11 +724,11 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
   for (int v = 0; v < NV; ++v) cap_total += cap[v];
   if (cap_total > (1ll << 31) - 1) throw Error(PPM_E_RANGE, "batch too large for one work queue");
   B.d_prof = (DevProfile*)B.mem.alloc(sizeof(DevProfile) * (size_t)n);
-  B.d_flux = (double*)B.mem.alloc(sizeof(double) * (size_t)std::max(1ll, B.flux_off[n]));
-  B.d_comp = (double*)B.mem.alloc(sizeof(double) * (size_t)std::max(1ll, B.flux_off[n]));
+  // the flux pool and its compensation pool in one block (cleared by one memset per pass)
+  B.d_flux = (double*)B.mem.alloc(2 * sizeof(double) * (size_t)std::max(1ll, B.flux_off[n]));
+  B.d_comp = B.d_flux + std::max(1ll, B.flux_off[n]);
   B.d_counts = (double*)B.mem.alloc(sizeof(double) * (size_t)std::max(1ll, B.counts_off[n]));
   Tile* tiles = (Tile*)B.mem.alloc(sizeof(Tile) * (size_t)std::max(1ll, cap_total));
-  B.d_ctrl = (int*)B.mem.alloc(sizeof(int) * 16);
   if (copy_stream)  // pageable source: returns once staged, ordered on the batch's stream
     PPM_CUDA(cudaMemcpyAsync(B.d_prof, hp.data(), sizeof(DevProfile) * (size_t)n, cudaMemcpyHostToDevice, copy_stream));
   else
@@ -800,11 +807,8 @@ void Engine::batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events) {
   if (events) PPM_CUDA(cudaEventRecord(events[0], st));
   {
     NvtxRange range("clear + plan");
-    PPM_CUDA(cudaMemsetAsync(B.d_flux, 0, sizeof(double) * (size_t)B.flux_off[n], st));
-    PPM_CUDA(cudaMemsetAsync(B.d_comp, 0, sizeof(double) * (size_t)B.flux_off[n], st));
-    PPM_CUDA(cudaMemsetAsync(B.d_stats, 0, sizeof(unsigned long long) * kStats * (size_t)n, st));
-    PPM_CUDA(cudaMemsetAsync(B.d_ring_seen, 0, sizeof(unsigned) * (size_t)B.ring_words, st));
-    PPM_CUDA(cudaMemsetAsync(B.d_ctrl, 0, sizeof(int) * 16, st));
+    PPM_CUDA(cudaMemsetAsync(B.d_flux, 0, 2 * sizeof(double) * (size_t)std::max(1ll, B.flux_off[n]), st));
+    PPM_CUDA(cudaMemsetAsync(B.d_stats, 0, B.small_bytes, st));
     for (const auto& G : B.groups)
       PPM_CUDA(launch_plan(B.d_prof + G.g0, G.g1 - G.g0, lens, G.args.queue, G.chunk, G.npt, st));
   }
@@ -1089,7 +1093,7 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
   nt = std::max(64, std::min(512, nt));
   // few energies: the blackbody kernel evaluates one phase point per thread
   // (its point-wise path, n_e * 4 <= threads), so size the block by points
-  if (!nsx_kernel && ne_max * 4 <= 256) nt = 256;
+  if (!nsx_kernel && ne_max * 4 <= 256) nt = tune.bb_nt > 0 ? tune.bb_nt : 256;
   // whole multiples of the warp count keep the one-warp-per-point build balanced
   const int nwarps = nt / 32;
   int pb = std::max(nwarps, (std::min(tune.pb, nt) / nwarps) * nwarps);

@@ -142,6 +142,7 @@ struct BatchImpl {
   double* d_counts = nullptr;
   unsigned* d_ring_seen = nullptr;  // ring bits behind the rings-with-active-elements counter
   long long ring_words = 0;
+  size_t small_bytes = 0;           // d_stats, d_ring_seen and d_ctrl: one block
   unsigned long long* d_stats = nullptr;
   int* d_ctrl = nullptr;
   FoldJob* d_jobs = nullptr;
@@ -200,6 +201,7 @@ struct Tuning {
   int sets = 0;      // home-cell kernel: warp sets per CTA (0 = about 256 threads)
   int cpl = 0;       // home-cell kernel: cells per lane (0 = by estimated cost)
   int splits = 0;    // phase-node splits per element chunk (0 = by the batch's work)
+  int bb_nt = 0;     // blackbody point paths (<= 64 energies): threads per CTA (0 = 256)
 };
 
 // Observed counts [n_ch][n_bins] for fit statistics.
