@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (profiling runs)")
     ap.add_argument("--probe-ranks", action="store_true",
                     help="check the rank launch only: every rank joins a gloo group and prints its rank and the "
                          "group size (no GPU work)")
@@ -323,7 +324,7 @@ def main():
     n = len(plist)
 
     # launch shape chosen by the autotuner on a sample of the same workload (outside the timed region)
-    tune_report = eng.autotune(plist[: min(128, n)])
+    tune_report = "" if args.no_autotune else eng.autotune(plist[: min(128, n)])
     chosen = [ln for ln in tune_report.splitlines() if ln.endswith("(chosen)")]
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
