@@ -1093,7 +1093,9 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
   nt = std::max(64, std::min(512, nt));
   // few energies: the blackbody kernel evaluates one phase point per thread
   // (its point-wise path, n_e * 4 <= threads), so size the block by points
-  if (!nsx_kernel && ne_max * 4 <= 256) nt = tune.bb_nt > 0 ? tune.bb_nt : 256;
+  // (512 threads for the phase-major walk, 4 energies or fewer: more segments of a ring in flight, half as many
+  // CTA slots to fill with a one-profile batch's rings)
+  if (!nsx_kernel && ne_max * 4 <= 256) nt = tune.bb_nt > 0 ? tune.bb_nt : (ne_max <= 4 ? 512 : 256);
   // whole multiples of the warp count keep the one-warp-per-point build balanced
   const int nwarps = nt / 32;
   int pb = std::max(nwarps, (std::min(tune.pb, nt) / nwarps) * nwarps);

@@ -201,7 +201,7 @@ struct Tuning {
   int sets = 0;      // home-cell kernel: warp sets per CTA (0 = about 256 threads)
   int cpl = 0;       // home-cell kernel: cells per lane (0 = by estimated cost)
   int splits = 0;    // phase-node splits per element chunk (0 = by the batch's work)
-  int bb_nt = 0;     // blackbody point paths (<= 64 energies): threads per CTA (0 = 256)
+  int bb_nt = 0;     // blackbody point paths (<= 64 energies): threads per CTA (0 = 512 up to 4 energies, else 256)
 };
 
 // Observed counts [n_ch][n_bins] for fit statistics.

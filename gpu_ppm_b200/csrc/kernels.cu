@@ -1087,6 +1087,11 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
       Real* E_s = (Real*)(inv_dp + n_fine);
       double* invE_s = (double*)(((uintptr_t)(E_s + n_e) + 7) & ~(uintptr_t)7);
       const bool staged = (long)((unsigned char*)(invE_s + n_e) - (unsigned char*)s.rows) <= (long)(S.total - S.off_rows);
+      // the phase-major walk also stages each active element's phase shift phi / 2 pi (one division per element
+      // per tile instead of one per element and node)
+      double* shift_s = invE_s + n_e;
+      const bool pm = n_e <= kPhaseMajorMaxE && mono &&
+                      (long)((unsigned char*)(shift_s + n_act) - (unsigned char*)s.rows) <= (long)(S.total - S.off_rows);
       if (staged) {
         if (mono)
           for (int i = tid; i < n_fine; i += nt) inv_dp[i] = 1.0 / (s.P[i + 1] - s.P[i]);
@@ -1094,13 +1099,15 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
           E_s[e] = (Real)G.E[e];
           invE_s[e] = G.invE[e];
         }
+        if (pm)
+          for (int jj = tid; jj < n_act; jj += nt) shift_s[jj] = (point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs)) / kTwoPi;
       }
       __syncthreads();
       const double* inv_dp_use = (staged && mono) ? inv_dp : nullptr;
       const int n_fp = n_fine + 1;
       const double P0 = s.P[0];
       const Real inv_kT = (Real)1 / kT;
-      if (n_e <= kPhaseMajorMaxE && staged && mono) {
+      if (pm && staged) {
         // Phase-major walk (the os1 light curves: one energy).  A work item is
         // one phase point and a contiguous segment of the tile's active
         // elements.  The elements' azimuths increase along the ring, so the
@@ -1139,8 +1146,7 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
           for (int e = 0; e < kPhaseMajorMaxE; ++e) acc[e] = 0.0;
           int hint = -1;
           for (int jj = jj0; jj < jj1; ++jj) {
-            const double phase_shift = (point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs)) / kTwoPi;
-            const double xph = ppt + phase_shift + 1.;
+            const double xph = ppt + shift_s[jj] + 1.;
             double patch = xph - floor(xph);
             if (patch < P0) patch += 1.;
             hint = hunt_from(s.P, n_fp, patch, hint);

@@ -99,7 +99,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--repeats", type=int, default=3)
     ap.add_argument("--layout", help="only write the reference program's working directory here and exit")
-    ap.add_argument("--only", help="scenario name for --layout")
+    ap.add_argument("--only", help="scenario name: for --layout, or the one star the engine runs (--program os1)")
     ap.add_argument("--program", default="all", choices=("devarshi", "os1", "all"))
     args = ap.parse_args()
     if args.layout:
@@ -168,6 +168,8 @@ def os1(args):
     eng.load_lensing(lens)
     g = eng.add_energy_grid(np.array([1.0]))
     for name, nu, th, inc, ar, beam in OS1:
+        if args.only and name != args.only:
+            continue
         row = {"scenario": name, "reference_gpu_ms": ref_ms[name], "repeats": args.repeats}
         for prec, tag in ((_abi.PREC_FP32, "fp32"), (_abi.PREC_FP64, "fp64")):
             kind = _abi.SPOT_POINT if ar < 0.1 else _abi.SPOT_HEALPIX
