@@ -27,6 +27,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -1013,6 +1014,58 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
 }
 
 // ---------------------------------------------------------------------------
+// The blackbody phase-major walk over the tile's elements jj0 .. jj1 - 1 at one
+// phase node (phase ppt, weight wgl): adds each visible element's Ibb at the
+// grid's first NE energies (NE = 1, or up to n_e) into acc and returns the
+// number of visible elements.  The patch phase and its phase_o bracket are
+// FP64 in every arithmetic, the bracket hunted from the previous element's.
+// FP64 arithmetic lerps F and Z in FP64 and divides exactly; FP32 arithmetic
+// lerps the tile's FP32 copies of F and Z and divides with the fast
+// reciprocal.
+template <typename Real, int NE>
+__device__ __forceinline__ unsigned pm_walk(const SmemPtrs& s, const double* inv_dp, const float* F32, const float* Z32,
+                                            const double* shift_s, const Real* E_s, int n_e, Real inv_kT, double ppt,
+                                            double wgl, int jj0, int jj1, int n_fp, double P0, double* acc) {
+  unsigned n_vis = 0;
+  int hint = -1;
+  for (int jj = jj0; jj < jj1; ++jj) {
+    const double xph = ppt + shift_s[jj] + 1.;
+    double patch = xph - floor(xph);
+    if (patch < P0) patch += 1.;
+    hint = hunt_from(s.P, n_fp, patch, hint);
+    const int i = clampi(hint, 0, n_fp - 2);
+    Real cb, zb;
+    if constexpr (std::is_same<Real, float>::value) {
+      const float af = (float)((patch - s.P[i]) * inv_dp[i]);
+      const float f0 = F32[i];
+      const float flux = fmaf(af, F32[i + 1] - f0, f0);
+      if (flux == 0.f) continue;
+      const float z0 = Z32[i];
+      zb = fmaf(af, Z32[i + 1] - z0, z0);
+      cb = flux * (float)wgl;
+    } else {
+      const double af = (patch - s.P[i]) * inv_dp[i];
+      const double flux = (1 - af) * s.F[i] + af * s.F[i + 1];
+      if (flux == 0) continue;
+      zb = (1 - af) * s.Z[i] + af * s.Z[i + 1];
+      cb = flux * wgl;
+    }
+    ++n_vis;
+#pragma unroll
+    for (int e = 0; e < NE; ++e)
+      if (NE == 1 || e < n_e) {
+        const Real Ee = E_s[e] * zb;
+        Real v;  // Ibb without its constant
+        if constexpr (std::is_same<Real, float>::value)
+          v = cb * __fdividef(Ee * Ee * Ee, expm1f(Ee * inv_kT));
+        else
+          v = cb * (Ee * Ee * Ee / expm1(Ee * inv_kT));
+        acc[e] += (double)v;
+      }
+  }
+  return n_vis;
+}
+
 template <typename Real, int NE_T>
 __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
@@ -1090,8 +1143,13 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
       // the phase-major walk also stages each active element's phase shift phi / 2 pi (one division per element
       // per tile instead of one per element and node)
       double* shift_s = invE_s + n_e;
+      // FP32 arithmetic: FP32 copies of the fine-phase F and Z after them
+      float* F32 = (float*)(shift_s + n_act);
+      float* Z32 = F32 + (n_fine + 1);
+      const bool fp32 = std::is_same<Real, float>::value;
       const bool pm = n_e <= kPhaseMajorMaxE && mono &&
-                      (long)((unsigned char*)(shift_s + n_act) - (unsigned char*)s.rows) <= (long)(S.total - S.off_rows);
+                      (long)((unsigned char*)(fp32 ? (void*)(Z32 + n_fine + 1) : (void*)(shift_s + n_act)) -
+                             (unsigned char*)s.rows) <= (long)(S.total - S.off_rows);
       if (staged) {
         if (mono)
           for (int i = tid; i < n_fine; i += nt) inv_dp[i] = 1.0 / (s.P[i + 1] - s.P[i]);
@@ -1099,8 +1157,14 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
           E_s[e] = (Real)G.E[e];
           invE_s[e] = G.invE[e];
         }
-        if (pm)
+        if (pm) {
           for (int jj = tid; jj < n_act; jj += nt) shift_s[jj] = (point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs)) / kTwoPi;
+          if (fp32)
+            for (int i = tid; i <= n_fine; i += nt) {
+              F32[i] = (float)s.F[i];
+              Z32[i] = (float)s.Z[i];
+            }
+        }
       }
       __syncthreads();
       const double* inv_dp_use = (staged && mono) ? inv_dp : nullptr;
@@ -1144,26 +1208,10 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
           double acc[kPhaseMajorMaxE];
 #pragma unroll
           for (int e = 0; e < kPhaseMajorMaxE; ++e) acc[e] = 0.0;
-          int hint = -1;
-          for (int jj = jj0; jj < jj1; ++jj) {
-            const double xph = ppt + shift_s[jj] + 1.;
-            double patch = xph - floor(xph);
-            if (patch < P0) patch += 1.;
-            hint = hunt_from(s.P, n_fp, patch, hint);
-            const int i = clampi(hint, 0, n_fp - 2);
-            const double af = (patch - s.P[i]) * inv_dp[i];
-            const double flux = (1 - af) * s.F[i] + af * s.F[i + 1];
-            if (flux == 0) continue;
-            const double z = (1 - af) * s.Z[i] + af * s.Z[i + 1];
-            ++n_vis;
-            const Real cb = (Real)(flux * wgl), zb = (Real)z;
-#pragma unroll
-            for (int e = 0; e < kPhaseMajorMaxE; ++e)
-              if (e < n_e) {
-                const Real Ee = E_s[e] * zb;
-                acc[e] += (double)(cb * (Ee * Ee * Ee / expm1(Ee * inv_kT)));  // Ibb without its constant
-              }
-          }
+          n_vis += n_e == 1 ? pm_walk<Real, 1>(s, inv_dp, F32, Z32, shift_s, E_s, n_e, inv_kT, ppt, wgl, jj0, jj1, n_fp,
+                                               P0, acc)
+                            : pm_walk<Real, kPhaseMajorMaxE>(s, inv_dp, F32, Z32, shift_s, E_s, n_e, inv_kT, ppt, wgl,
+                                                             jj0, jj1, n_fp, P0, acc);
 #pragma unroll
           for (int e = 0; e < kPhaseMajorMaxE; ++e)
             if (e < n_e && acc[e] != 0.0) {
