@@ -229,6 +229,39 @@ def test_chunked_rings_and_small_batches(monkeypatch):
     e.close()
 
 
+def test_node_splits_give_the_same_bits(monkeypatch):
+    """The NSX home-cell kernel's tiles may split a ring chunk's phase nodes
+    into any number of ranges (PPM_SPLITS forces 1, 3 or 16): every node's
+    partial sums are formed the same way and the flux additions are
+    compensated, so the flux and counts are the same bits; the blackbody
+    kernel, which also sums in FP64, agrees to 1e-12."""
+    lens, nsx = synth.lensing("std"), synth.nsx("v171019", seed=0)
+    E = synth.energy_grid(300, 0.2, 12.0)
+    rsp = synth.response(300, 1000, E, seed=0)
+    E_bb = synth.energy_grid(3, 0.5, 4.0)
+    out = {}
+    for splits in ("1", "3", "16"):
+        monkeypatch.setenv("PPM_SPLITS", splits)
+        e = Engine()
+        try:
+            e.load_lensing(lens)
+            e.load_nsx(nsx)
+            g = e.add_energy_grid(E)
+            r = e.add_response(g, rsp)
+            g_bb = e.add_energy_grid(E_bb)
+            plist, _ = synth.draw_prior(3, seed=7, lens_u=(0.3, 0.5), n_side=48, n_bins=32, energy_grid=g, response=r)
+            bb = synth.config1_params(g_bb)
+            bb.precision = _abi.PREC_FP32
+            out[splits] = ([e.profile(p)[:2] for p in plist], e.profile(bb)[0])
+        finally:
+            e.close()
+    for splits in ("3", "16"):
+        for (f0, c0), (f1, c1) in zip(out["1"][0], out[splits][0]):
+            assert np.array_equal(f0, f1), (splits, max_rel(f1, f0))
+            assert np.array_equal(c0, c1), (splits, max_rel(c1, c0))
+        assert max_rel(out[splits][1], out["1"][1]) < 1e-12, splits
+
+
 def test_autotune_keeps_parity(eng_v171019):
     g, r, E, rsp = eng_v171019.cfg2
     plist, _ = synth.draw_prior(8, seed=21, lens_u=(0.3, 0.5), n_side=32, n_bins=16, energy_grid=g, response=r)
