@@ -1032,6 +1032,10 @@ __device__ __forceinline__ unsigned pm_walk(const SmemPtrs& s, const double* inv
     const double xph = ppt + shift_s[jj] + 1.;
     double patch = xph - floor(xph);
     if (patch < P0) patch += 1.;
+    // phase_o[i] is phase i / n_fine plus a small time-of-flight delay: the
+    // first element's hunt starts from that guess, the others from the
+    // previous bracket
+    if (hint < 0) hint = clampi((int)(patch * (n_fp - 1)), 0, n_fp - 2);
     hint = hunt_from(s.P, n_fp, patch, hint);
     const int i = clampi(hint, 0, n_fp - 2);
     Real cb, zb;
@@ -1158,6 +1162,7 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
           invE_s[e] = G.invE[e];
         }
         if (pm) {
+          if (tid == 0) s_int[47] = 0;  // work items taken (phase-major walk)
           for (int jj = tid; jj < n_act; jj += nt) shift_s[jj] = (point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs)) / kTwoPi;
           if (fp32)
             for (int i = tid; i <= n_fine; i += nt) {
@@ -1182,11 +1187,21 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
         // per energy flushes them at the end of the segment.
         const int n_gl = p.n_gl;
         const double inv_bins = 1. / p.n_bins;
-        const int segs = max(1, min(n_act, nt / max(1, n_pp)));
+        // about four items per thread, taken 32 at a time by each warp from a
+        // shared counter: nodes where the element is hidden finish early, and
+        // their warps take more items instead of waiting at the next tile
+        const int segs = max(1, min(n_act, 4 * nt / max(1, n_pp)));
         const int n_items = n_pp * segs;
         const double scale = out_scale;
+        const int lane = tid & 31;
         unsigned int n_vis = 0;
-        for (int it = tid; it < n_items; it += nt) {
+        for (;;) {
+          int base = 0;
+          if (lane == 0) base = atomicAdd(&s_int[47], 32);
+          base = __shfl_sync(0xffffffffu, base, 0);
+          if (base >= n_items) break;
+          const int it = base + lane;
+          if (it >= n_items) continue;
           const int k = tile.u0 + it % n_pp, seg = it / n_pp;
           const int jj0 = (int)((long long)n_act * seg / segs), jj1 = (int)((long long)n_act * (seg + 1) / segs);
           int bin, g = 0;
@@ -1219,7 +1234,6 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
               comp_add(flux_base + o, comp_base ? comp_base + o : nullptr, acc[e] * scale * invE_s[e]);
             }
         }
-        const int lane = tid & 31;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) n_vis += __shfl_down_sync(0xffffffffu, n_vis, off);
         if (lane == 0 && n_vis) atomicAdd(&p.stats[3], (unsigned long long)n_vis);
