@@ -1162,7 +1162,6 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
           invE_s[e] = G.invE[e];
         }
         if (pm) {
-          if (tid == 0) s_int[47] = 0;  // work items taken (phase-major walk)
           for (int jj = tid; jj < n_act; jj += nt) shift_s[jj] = (point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs)) / kTwoPi;
           if (fp32)
             for (int i = tid; i <= n_fine; i += nt) {
@@ -1187,21 +1186,16 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
         // per energy flushes them at the end of the segment.
         const int n_gl = p.n_gl;
         const double inv_bins = 1. / p.n_bins;
-        // about four items per thread, taken 32 at a time by each warp from a
-        // shared counter: nodes where the element is hidden finish early, and
-        // their warps take more items instead of waiting at the next tile
-        const int segs = max(1, min(n_act, 4 * nt / max(1, n_pp)));
+        // one item per thread (as many segments per node as the block has
+        // threads per node): each item ends with one compensated atomic per
+        // energy, whose returned value the thread waits for, so items are
+        // kept few and long
+        const int segs = max(1, min(n_act, nt / max(1, n_pp)));
         const int n_items = n_pp * segs;
         const double scale = out_scale;
         const int lane = tid & 31;
         unsigned int n_vis = 0;
-        for (;;) {
-          int base = 0;
-          if (lane == 0) base = atomicAdd(&s_int[47], 32);
-          base = __shfl_sync(0xffffffffu, base, 0);
-          if (base >= n_items) break;
-          const int it = base + lane;
-          if (it >= n_items) continue;
+        for (int it = tid; it < n_items; it += nt) {
           const int k = tile.u0 + it % n_pp, seg = it / n_pp;
           const int jj0 = (int)((long long)n_act * seg / segs), jj1 = (int)((long long)n_act * (seg + 1) / segs);
           int bin, g = 0;
