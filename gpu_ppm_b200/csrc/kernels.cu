@@ -1027,20 +1027,19 @@ __device__ __forceinline__ unsigned pm_walk(const SmemPtrs& s, const double* inv
                                             const double* shift_s, const Real* E_s, int n_e, Real inv_kT, double ppt,
                                             double wgl, int jj0, int jj1, int n_fp, double P0, double* acc) {
   unsigned n_vis = 0;
-  int j = -2;  // largest index with phase_o[j] <= patch (-1: below phase_o[0]), from the previous element
+  int hint = -1;
   for (int jj = jj0; jj < jj1; ++jj) {
     const double xph = ppt + shift_s[jj] + 1.;
     // x - floor(x) for x in [1, 3]: the same exact value
     double patch = xph - (xph >= 3.0 ? 3.0 : (xph >= 2.0 ? 2.0 : 1.0));
     if (patch < P0) patch += 1.;
     // phase_o[i] is phase i / n_fine plus a small time-of-flight delay: the
-    // first element starts from that guess, the others from the previous
-    // bracket, which moves by about one fine sample every few elements; a
-    // walk forward then back gives vhunt's bracket on a non-decreasing phase_o
-    if (j < -1) j = clampi((int)(patch * (n_fp - 1)), 0, n_fp - 1);
-    while (j + 1 < n_fp && patch >= s.P[j + 1]) ++j;
-    while (j >= 0 && patch < s.P[j]) --j;
-    const int i = clampi(j, 0, n_fp - 2);
+    // first element's hunt starts from that guess, the others from the
+    // previous bracket (by doubling steps: one or two for the next element,
+    // a few when the patch phase wraps past 1)
+    if (hint < 0) hint = clampi((int)(patch * (n_fp - 1)), 0, n_fp - 2);
+    hint = hunt_from(s.P, n_fp, patch, hint);
+    const int i = clampi(hint, 0, n_fp - 2);
     Real cb, zb;
     if constexpr (std::is_same<Real, float>::value) {
       const float af = (float)((patch - s.P[i]) * inv_dp[i]);
