@@ -1181,9 +1181,9 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
       const double P0 = s.P[0];
       const Real inv_kT = (Real)1 / kT;
       if (pm && staged) {
-        // Phase-major walk (the os1 light curves: one energy).  A work item is
-        // one phase point and a contiguous segment of the tile's active
-        // elements.  The elements' azimuths increase along the ring, so the
+        // Phase-major walk (the os1 light curves: one energy).  A thread walks
+        // a contiguous segment of the tile's active elements at one phase
+        // point, then at a second one.  The elements' azimuths increase along the ring, so the
         // point's patch phase moves monotonically from one element to the
         // next (wrapping once past 1) and its phase_o bracket is hunted from
         // the previous element's: vhunt's bracket exactly, as phase_o is
@@ -1191,47 +1191,54 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
         // per energy flushes them at the end of the segment.
         const int n_gl = p.n_gl;
         const double inv_bins = 1. / p.n_bins;
-        // one item per thread (as many segments per node as the block has
-        // threads per node): each item ends with one compensated atomic per
-        // energy, whose returned value the thread waits for, so items are
-        // kept few and long
-        const int segs = max(1, min(n_act, nt / max(1, n_pp)));
-        const int n_items = n_pp * segs;
+        // Work items pair node k with node k + H, H = ceil(nodes / 2), half a
+        // rotation later, on one segment: an element seen at one of the two
+        // phases is often hidden at the other, so the pairs cost about the
+        // same and the warps finish together.  Each item ends with one
+        // compensated atomic per energy, whose returned value the thread
+        // waits for, so the items are kept few and long.
+        const int H = (n_pp + 1) / 2;
+        const int segs = max(1, min(n_act, nt / max(1, H)));
         const double scale = out_scale;
         const int lane = tid & 31;
         unsigned int n_vis = 0;
-        for (int it = tid; it < n_items; it += nt) {
-          const int k = tile.u0 + it % n_pp, seg = it / n_pp;
+        for (int it = tid; it < H * segs; it += nt) {
+          const int seg = it / H;
           const int jj0 = (int)((long long)n_act * seg / segs), jj1 = (int)((long long)n_act * (seg + 1) / segs);
-          int bin, g = 0;
-          if (n_gl > 0) {
-            bin = k / n_gl;
-            g = k - bin * n_gl;
-          } else {
-            bin = k;
-          }
-          double ppt, wgl;
-          if (n_gl > 0) {
-            const double lb = bin * inv_bins, ub = (bin + 1) * inv_bins;
-            ppt = 0.5 * (lb + ub + c_gl_nodes[n_gl * (n_gl - 1) / 2 + g] * (ub - lb));
-            wgl = 0.5 * 1. * c_gl_weights[n_gl * (n_gl - 1) / 2 + g];
-          } else {
-            ppt = bin * inv_bins;
-            wgl = 1.0;
-          }
-          double acc[kPhaseMajorMaxE];
-#pragma unroll
-          for (int e = 0; e < kPhaseMajorMaxE; ++e) acc[e] = 0.0;
-          n_vis += n_e == 1 ? pm_walk<Real, 1>(s, inv_dp, F32, Z32, shift_s, E_s, n_e, inv_kT, ppt, wgl, jj0, jj1, n_fp,
-                                               P0, acc)
-                            : pm_walk<Real, kPhaseMajorMaxE>(s, inv_dp, F32, Z32, shift_s, E_s, n_e, inv_kT, ppt, wgl,
-                                                             jj0, jj1, n_fp, P0, acc);
-#pragma unroll
-          for (int e = 0; e < kPhaseMajorMaxE; ++e)
-            if (e < n_e && acc[e] != 0.0) {
-              const size_t o = (size_t)bin * n_e + e;
-              comp_add(flux_base + o, comp_base ? comp_base + o : nullptr, acc[e] * scale * invE_s[e]);
+          for (int half = 0; half < 2; ++half) {
+            const int kk = it % H + half * H;
+            if (kk >= n_pp) break;
+            const int k = tile.u0 + kk;
+            int bin, g = 0;
+            if (n_gl > 0) {
+              bin = k / n_gl;
+              g = k - bin * n_gl;
+            } else {
+              bin = k;
             }
+            double ppt, wgl;
+            if (n_gl > 0) {
+              const double lb = bin * inv_bins, ub = (bin + 1) * inv_bins;
+              ppt = 0.5 * (lb + ub + c_gl_nodes[n_gl * (n_gl - 1) / 2 + g] * (ub - lb));
+              wgl = 0.5 * 1. * c_gl_weights[n_gl * (n_gl - 1) / 2 + g];
+            } else {
+              ppt = bin * inv_bins;
+              wgl = 1.0;
+            }
+            double acc[kPhaseMajorMaxE];
+#pragma unroll
+            for (int e = 0; e < kPhaseMajorMaxE; ++e) acc[e] = 0.0;
+            n_vis += n_e == 1 ? pm_walk<Real, 1>(s, inv_dp, F32, Z32, shift_s, E_s, n_e, inv_kT, ppt, wgl, jj0, jj1,
+                                                 n_fp, P0, acc)
+                              : pm_walk<Real, kPhaseMajorMaxE>(s, inv_dp, F32, Z32, shift_s, E_s, n_e, inv_kT, ppt, wgl,
+                                                               jj0, jj1, n_fp, P0, acc);
+#pragma unroll
+            for (int e = 0; e < kPhaseMajorMaxE; ++e)
+              if (e < n_e && acc[e] != 0.0) {
+                const size_t o = (size_t)bin * n_e + e;
+                comp_add(flux_base + o, comp_base ? comp_base + o : nullptr, acc[e] * scale * invE_s[e]);
+              }
+          }
         }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) n_vis += __shfl_down_sync(0xffffffffu, n_vis, off);
