@@ -836,6 +836,7 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
     const bool sg = mode == 1;
     const int ST = 32 * S.cell_warps;  // threads of a set
     const int st = tid - set * ST;     // this thread's index in its set
+    const bool lane_cells = lane < kOwners && r0 < G.span;  // the lane owns cells of the grid
     float4* srec = rec + 2 * set * ST;  // the set's records
     if (lane == 0) {
       s_nvis[warp] = 0;
@@ -943,14 +944,27 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
 #pragma unroll
             for (int i = 0; i <= C; ++i) Q[i] = make_float4(h[i + 1], h[i + 2] - h[i + 1], 0.f, 0.f);
           }
-          // cells past an end hold the end value: H[0] is h[i] there; H[nE - 1]
-          // is h[i + 1], except where that window row is the extrapolated row nE
-          if (__any_sync(0xffffffffu, g < 0 || g + C > nE - 2)) {
+          // cells past an end hold the end value.  A cell four or more rows past
+          // an end reads four equal clamped rows, so its cubic is that constant
+          // already; the three cells next to each end become constants here.
+          // Their value is the x of a cubic (the x of cell k is row k): of the
+          // cell itself, except for cell nE and cell -1, whose rows are the
+          // extrapolated ones; they take the x of a neighbouring cell, row
+          // nE + 1 or nE - 1 (both hold H[nE - 1]), row 0 or row -2 (H[0]).
+          if (__any_sync(0xffffffffu, lane_cells && g + C >= nE - 1 && g <= nE + 1)) {
 #pragma unroll
             for (int i = 0; i <= C; ++i) {
               const int gi = g + i;
-              if (gi < 0) Q[i] = make_float4(h[i], 0.f, 0.f, 0.f);
-              if (gi > nE - 2) Q[i] = make_float4(gi == nE ? h[i] : h[i + 1], 0.f, 0.f, 0.f);
+              const float nb = i < C ? Q[i + 1].x : Q[i > 0 ? i - 1 : 0].x;
+              if ((unsigned)(gi - (nE - 1)) <= 2u) Q[i] = make_float4(gi == nE ? nb : Q[i].x, 0.f, 0.f, 0.f);
+            }
+          }
+          if (__any_sync(0xffffffffu, lane_cells && g <= -1 && g + C >= -3)) {
+#pragma unroll
+            for (int i = 0; i <= C; ++i) {
+              const int gi = g + i;
+              const float nb = i < C ? Q[i + 1].x : Q[i > 0 ? i - 1 : 0].x;
+              if ((unsigned)(gi + 3) <= 2u) Q[i] = make_float4(gi == -1 ? nb : Q[i].x, 0.f, 0.f, 0.f);
             }
           }
           const f32x2 cw2 = pk(rA.x, rA.x), fP2 = pk(rA.y, rA.y), m1 = pk(-1.f, -1.f);
