@@ -196,6 +196,15 @@ __host__ __device__ __forceinline__ int hunt_from(const double* xx, int n, doubl
   return lo;
 }
 
+// vhunt's clamped bracket on a non-decreasing xx (the largest i <= n - 2 with
+// xx[i] <= x, or 0) by unit steps from any i in [0, n - 2]: a step or none
+// when i is the bracket of a nearby x.
+__host__ __device__ __forceinline__ int walk_bracket(const double* xx, int n, double x, int i) {
+  while (i > 0 && x < xx[i]) --i;
+  while (i < n - 2 && x >= xx[i + 1]) ++i;
+  return i;
+}
+
 // cpu/nsx.hpp:159-168
 __device__ __forceinline__ void cubic_lagrange(double w[4], double x, double x0, double x1, double x2, double x3) {
   w[0] = (x - x1) * (x - x2) * (x - x3) / ((x0 - x1) * (x0 - x2) * (x0 - x3));

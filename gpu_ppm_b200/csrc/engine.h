@@ -281,8 +281,9 @@ class Engine {
   DevGrid dev_grid(int id);
   const double* ring_table(int N);
   const double* fine_table(int nf);
+  // rings: rings the group's spots span (sizes the blackbody phase-major walk's blocks; 0 = unknown)
   IntegrandShape choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, int nf_max, int cells_max, int maxe_max = 0,
-                              int bins_max = 0, bool allow_cell = true);
+                              int bins_max = 0, bool allow_cell = true, double rings = 0);
   bool cell_kernel_takes(int grid);
   void group_tiling(bool pooled, const GroupWork& w, int chunk_override, int* chunk, int* npt) const;
   long long tile_bound(const ppm_params& p, const DevProfile& d, int chunk, int npt) const;

@@ -1042,18 +1042,23 @@ __device__ __forceinline__ unsigned pm_walk(const SmemPtrs& s, const double* inv
                                             double wgl, int jj0, int jj1, int n_fp, double P0, double* acc) {
   unsigned n_vis = 0;
   int hint = -1;
+  double prev = -1.0;  // below every patch phase
   for (int jj = jj0; jj < jj1; ++jj) {
     const double xph = ppt + shift_s[jj] + 1.;
     // x - floor(x) for x in [1, 3]: the same exact value
     double patch = xph - (xph >= 3.0 ? 3.0 : (xph >= 2.0 ? 2.0 : 1.0));
     if (patch < P0) patch += 1.;
     // phase_o[i] is phase i / n_fine plus a small time-of-flight delay: the
-    // first element's hunt starts from that guess, the others from the
-    // previous bracket (by doubling steps: one or two for the next element,
-    // a few when the patch phase wraps past 1)
-    if (hint < 0) hint = clampi((int)(patch * (n_fp - 1)), 0, n_fp - 2);
-    hint = hunt_from(s.P, n_fp, patch, hint);
-    const int i = clampi(hint, 0, n_fp - 2);
+    // first element's bracket is walked to from that guess, the others' from
+    // the previous bracket by unit steps (none or one for the next element;
+    // from the first bracket when the patch phase wraps past phase_o[0] + 1).
+    // On a non-decreasing phase_o the walk stops at vhunt's bracket: the
+    // largest i <= n - 2 with phase_o[i] <= patch, or 0.
+    if (patch < prev) hint = 0;
+    prev = patch;
+    if (hint < 0) hint = clampi((int)((patch - P0) * (n_fp - 1)), 0, n_fp - 2);
+    hint = walk_bracket(s.P, n_fp, patch, hint);
+    const int i = hint;
     Real cb, zb;
     if constexpr (std::is_same<Real, float>::value) {
       const float af = (float)((patch - s.P[i]) * inv_dp[i]);

@@ -1,6 +1,7 @@
 // Host check that hunt_from (the blackbody point-wise path's warm-started
-// phase_o hunt) brackets exactly as vhunt's bisection on non-decreasing
-// arrays, from any starting index: same clamped index, same fraction.
+// phase_o hunt) and walk_bracket (the phase-major walk's unit steps) bracket
+// exactly as vhunt's bisection on non-decreasing arrays, from any starting
+// index: same clamped index, same fraction.
 // Random arrays with repeated values, x inside, at and outside the nodes.
 // Built and run by tests/test_hunt.py; prints "<cases> <mismatches>".
 #include <cstdio>
@@ -29,9 +30,10 @@ int main() {
       const int i_ref = ppm::vhunt(xx.data(), n, x, a_ref);
       const int i = ppm::clampi(ppm::hunt_from(xx.data(), n, x, hint), 0, n - 2);
       const double a = (x - xx[i]) / (xx[i + 1] - xx[i]);
+      const int iw = ppm::walk_bracket(xx.data(), n, x, ppm::clampi(hint, 0, n - 2));
       ++cases;
       const bool same_a = (a == a_ref) || (a != a && a_ref != a_ref);
-      if (i != i_ref || !same_a) ++bad;
+      if (i != i_ref || !same_a || iw != i_ref) ++bad;
     }
   }
   std::printf("%lld %lld\n", cases, bad);

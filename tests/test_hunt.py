@@ -1,6 +1,7 @@
 """The blackbody point-wise path hunts phase_o from each thread's previous
-bracket (hunt_from, csrc/device.cuh); on a non-decreasing phase_o it must give
-the same clamped index and fraction as vhunt's bisection, from any start.
+bracket (hunt_from, csrc/device.cuh) and the phase-major walk steps to it
+(walk_bracket); on a non-decreasing phase_o both must give the same clamped
+index and fraction as vhunt's bisection, from any start.
 Checked on the host: tests/hunt_check.cu compiles the same device header with
 nvcc and compares both on random arrays with repeated values."""
 import os
