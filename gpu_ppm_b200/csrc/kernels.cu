@@ -931,6 +931,14 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
           srec[2 * slot] = make_float4(c, fP, __int_as_float(imu), __int_as_float(G0));
           srec[2 * slot + 1] = make_float4(w4[0], w4[1], w4[2], w4[3]);
         }
+        // whether a record of this step may use a cell next to the high or the low end of the table (cells
+        // G0 .. G0 + span are in use); the same for every lane: the warp's votes, or both ends for sets of
+        // several warps
+        bool step_hi = true, step_lo = true;
+        if (S.cell_warps == 1) {
+          step_hi = __any_sync(0xffffffffu, vis && G0 + G.span >= nE - 1 && G0 <= nE + 1);
+          step_lo = __any_sync(0xffffffffu, vis && G0 <= -1 && G0 + G.span >= -3);
+        }
         set_sync(set, ST);
         for (int b = 0; b < nv; ++b) {
           const float4 rA = srec[2 * b], wA = srec[2 * b + 1];
@@ -951,7 +959,7 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
           // cell itself, except for cell nE and cell -1, whose rows are the
           // extrapolated ones; they take the x of a neighbouring cell, row
           // nE + 1 or nE - 1 (both hold H[nE - 1]), row 0 or row -2 (H[0]).
-          if (__any_sync(0xffffffffu, lane_cells && g + C >= nE - 1 && g <= nE + 1)) {
+          if (step_hi && __any_sync(0xffffffffu, lane_cells && g + C >= nE - 1 && g <= nE + 1)) {
 #pragma unroll
             for (int i = 0; i <= C; ++i) {
               const int gi = g + i;
@@ -959,7 +967,7 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
               if ((unsigned)(gi - (nE - 1)) <= 2u) Q[i] = make_float4(gi == nE ? nb : Q[i].x, 0.f, 0.f, 0.f);
             }
           }
-          if (__any_sync(0xffffffffu, lane_cells && g <= -1 && g + C >= -3)) {
+          if (step_lo && __any_sync(0xffffffffu, lane_cells && g <= -1 && g + C >= -3)) {
 #pragma unroll
             for (int i = 0; i <= C; ++i) {
               const int gi = g + i;
