@@ -12,7 +12,10 @@ energies over 0.2-12 keV and a 300-channel response.
   (:452-483), read from its output; the first scenario is the program's warm-up.
 * engine device: one plan + integrand + fold pass of a one-profile batch,
   CUDA events around each phase (ppm_batch_launch_timed); the phases
-  (clear + plan, integrand, fold) are reported too.
+  (clear + plan, integrand, fold) are reported too.  The events between the
+  phases add their own gaps, so the pass is also timed whole: the batch's
+  captured graph (ppm_batch_launch) between two events, as the reference
+  times its kernel (engine graph).
 * engine plain: the synchronous ppm_profile call, host wall clock, counts
   downloaded to the host.
 
@@ -133,6 +136,16 @@ def engine_times(eng, prm, repeats, want_counts):
             dev.append(float(sum(ms3)))
             phases.append(list(ms3))
     engine_times.last_phases = [float(x) for x in np.median(np.array(phases), axis=0)]
+    graph = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for k in range(repeats + 1):
+        e0.record(stream)
+        _abi.check(_abi.lib().ppm_batch_launch(eng.h, batch.h, ctypes.c_void_p(stream.cuda_stream)))
+        e1.record(stream)
+        e1.synchronize()
+        if k:
+            graph.append(e0.elapsed_time(e1))
+    engine_times.last_graph = float(np.median(graph))
     batch.close()
     plain = []
     for k in range(repeats + 1):
@@ -180,6 +193,7 @@ def os1(args):
                                n_fine=384, energy_grid=g, precision=prec)
             dev, plain, flux, _ = engine_times(eng, prm, args.repeats, want_counts=False)
             row.update({f"engine_{tag}_device_ms": dev, f"engine_{tag}_plain_ms": plain,
+                        f"engine_{tag}_graph_ms": engine_times.last_graph,
                         f"engine_{tag}_phases_ms": engine_times.last_phases,
                         f"speedup_{tag}_device": ref_ms[name] / dev,
                         f"max_rel_diff_{tag}": max_rel(np.asarray(flux).reshape(-1), ref_flux[name])})
@@ -227,7 +241,7 @@ def devarshi(args):
         print(json.dumps({
             "scenario": name, "n_side": n_side, "energies": len(E), "channels": rsp.shape[0], "bins": 32,
             "reference_gpu_ms": ref, "engine_device_ms": dev, "engine_plain_ms": plain,
-            "engine_phases_ms": engine_times.last_phases,
+            "engine_graph_ms": engine_times.last_graph, "engine_phases_ms": engine_times.last_phases,
             "speedup_device": ref / dev, "speedup_plain": ref / plain,
             "max_rel_diff_counts": max_rel(counts.reshape(ref_counts[name].shape), ref_counts[name]),
             "repeats": args.repeats, "visible_points": int(info.n_points),
