@@ -660,15 +660,17 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
     B.counts_off[i + 1] = B.counts_off[i] + nc;
   }
   // kernel variants, one group and integrand launch each: 0 = NSX home-cell kernel, 1 = blackbody FP64,
-  // 2 = blackbody FP32, 3 = NSX pooled-polynomial kernel (grids the home-cell kernel does not take)
+  // 2 = blackbody FP32, 3 = NSX pooled-polynomial kernel (grids the home-cell kernel does not take), 4 = NSX
+  // home-cell kernel for grids with at most two energies in an NSX cell (half the energy slots of variant 0)
   std::map<int, bool> cell_ok;  // per energy grid
   auto variant = [&](const ppm_params& p) -> int {
     if (p.atmosphere != PPM_ATM_NSX) return p.precision == PPM_PREC_FP64 ? 1 : 2;
     auto it = cell_ok.find(p.energy_grid);
     if (it == cell_ok.end()) it = cell_ok.emplace(p.energy_grid, cell_kernel_takes(p.energy_grid)).first;
-    return it->second ? 0 : 3;
+    if (!it->second) return 3;
+    return grids[p.energy_grid].maxe <= 2 ? 4 : 0;
   };
-  constexpr int NV = 4;
+  constexpr int NV = 5;
   std::vector<int> order, vof(n);
   order.reserve(n);
   for (int i = 0; i < n; ++i) vof[i] = variant(ps[i]);
@@ -711,8 +713,8 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
   int chunk[NV], npt[NV];
   for (int v = 0; v < NV; ++v) group_tiling(v == 3, gw[v], chunk_override, &chunk[v], &npt[v]);
   B.chunk = chunk[0];
-  long long cap[NV] = {0, 0, 0, 0};
-  int start[NV + 1] = {0, 0, 0, 0, 0};
+  long long cap[NV] = {0, 0, 0, 0, 0};
+  int start[NV + 1] = {0, 0, 0, 0, 0, 0};
   for (int k = 0; k < n; ++k) {
     const int i = order[k];
     const int v = vof[i];
@@ -765,8 +767,10 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
     G.args.flux = B.d_flux;
     G.args.comp = B.d_comp;
     G.args.shape =
-        choose_shape(v == 0 || v == 3, v == 1, ne_max, nf_max, cells_max, maxe_max, bins_max, v == 0, gw[v].rings);
-    if (v == 0 && !G.args.shape.cellk) throw Error(PPM_E_STATE, "home-cell NSX kernel expected for the grid");
+        choose_shape(v == 0 || v == 3 || v == 4, v == 1, ne_max, nf_max, cells_max, maxe_max, bins_max,
+                     v == 0 || v == 4, gw[v].rings);
+    if ((v == 0 || v == 4) && !G.args.shape.cellk)
+      throw Error(PPM_E_STATE, "home-cell NSX kernel expected for the grid");
     PPM_CUDA(configure_integrand_smem(G.args.shape));
     const int occ = max_active_ctas(G.args.shape);
     if (occ < 1)
@@ -895,7 +899,7 @@ void Engine::batch_collect(BatchImpl& B, double* flux, double* counts, ppm_resul
   PPM_CUDA(cudaMemcpyAsync(ctrl, B.d_ctrl, sizeof(ctrl), cudaMemcpyDeviceToHost, st));
   PPM_CUDA(cudaStreamSynchronize(st));
   PPM_CUDA(cudaGetLastError());
-  if (ctrl[2] || ctrl[5] || ctrl[8] || ctrl[11]) throw Error(PPM_E_RANGE, "work queue overflow");
+  if (ctrl[2] || ctrl[5] || ctrl[8] || ctrl[11] || ctrl[14]) throw Error(PPM_E_RANGE, "work queue overflow");
   int err = 0;
   PPM_CUDA(cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) {
@@ -1045,12 +1049,12 @@ IntegrandShape Engine::choose_shape(bool nsx_kernel, bool bb_fp64, int ne_max, i
   // home-cell NSX kernel: cpl cells per lane (the last (cpl + 3) / cpl lanes of a warp
   // only supply slice rows), warp sets up to 512 threads
   const int span_max = cells_max - 1;
-  const int maxe_t = maxe_max <= 4 ? 4 : (maxe_max <= 8 ? 8 : 16);
+  const int maxe_t = maxe_max <= 2 ? 2 : (maxe_max <= 4 ? 4 : (maxe_max <= 8 ? 8 : 16));
   if (allow_cell && nsx_kernel && tune.kernel == 0 && maxe_max >= 1 && maxe_max <= 16 && span_max <= 16 * 32 &&
       nsx.nmu < 4096 && bins_max < (1 << 20)) {
     // cells per lane: fewest estimated lane instructions per point (window rows,
     // polynomials, record handling, energy slots), over what the slots' registers allow
-    const int cmax = maxe_t == 4 ? 3 : (maxe_t == 8 ? 2 : 1);
+    const int cmax = maxe_t <= 4 ? 3 : (maxe_t == 8 ? 2 : 1);
     int cpl = 1;
     long best = -1;
     auto cells_per_warp = [](int c) { return (32 - (c + 3) / c) * c; };  // lanes with home cells x c

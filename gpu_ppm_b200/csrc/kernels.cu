@@ -1620,6 +1620,11 @@ void* kernel_for(const IntegrandShape& s, int precision) {
   if (s.nsx && s.cellk) {
     // register budget: two CTAs per SM (80 registers) up to 384 threads, else one
     const bool two = s.minb >= 2 && s.nt <= 384;
+    if (s.maxe_t == 2) {
+      if (s.cpl >= 3) return two ? (void*)integrand_nsx_cell_kernel<2, 3, 384, 2> : (void*)integrand_nsx_cell_kernel<2, 3, 512, 1>;
+      if (s.cpl == 2) return two ? (void*)integrand_nsx_cell_kernel<2, 2, 384, 2> : (void*)integrand_nsx_cell_kernel<2, 2, 512, 1>;
+      return two ? (void*)integrand_nsx_cell_kernel<2, 1, 384, 2> : (void*)integrand_nsx_cell_kernel<2, 1, 512, 1>;
+    }
     if (s.maxe_t == 4) {
       if (s.cpl >= 3) return two ? (void*)integrand_nsx_cell_kernel<4, 3, 384, 2> : (void*)integrand_nsx_cell_kernel<4, 3, 512, 1>;
       if (s.cpl == 2) return two ? (void*)integrand_nsx_cell_kernel<4, 2, 384, 2> : (void*)integrand_nsx_cell_kernel<4, 2, 512, 1>;
@@ -1675,7 +1680,10 @@ cudaError_t once_per_device(int slot, cudaError_t (*set_up)()) {
 namespace {
 // every integrand variant gets the largest dynamic shared-memory allowance of the current device
 cudaError_t set_integrand_smem() {
-  void* fns[] = {(void*)integrand_nsx_cell_kernel<4, 1, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 1, 384, 2>,
+  void* fns[] = {(void*)integrand_nsx_cell_kernel<2, 1, 512, 1>, (void*)integrand_nsx_cell_kernel<2, 1, 384, 2>,
+                 (void*)integrand_nsx_cell_kernel<2, 2, 512, 1>, (void*)integrand_nsx_cell_kernel<2, 2, 384, 2>,
+                 (void*)integrand_nsx_cell_kernel<2, 3, 512, 1>, (void*)integrand_nsx_cell_kernel<2, 3, 384, 2>,
+                 (void*)integrand_nsx_cell_kernel<4, 1, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 1, 384, 2>,
                  (void*)integrand_nsx_cell_kernel<4, 2, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 2, 384, 2>,
                  (void*)integrand_nsx_cell_kernel<4, 3, 512, 1>, (void*)integrand_nsx_cell_kernel<4, 3, 384, 2>,
                  (void*)integrand_nsx_cell_kernel<8, 1, 512, 1>, (void*)integrand_nsx_cell_kernel<8, 1, 384, 2>,

@@ -23,7 +23,7 @@ struct IntegrandShape {
   int minb;       // CTAs per SM the register budget is compiled for (1 or 2)
   // home-cell NSX kernel: one lane per energy cell, record groups of cell_warps warps
   int cellk;      // 1 = home-cell kernel, 0 = pooled-polynomial kernel
-  int maxe_t;     // energies per lane the home-cell kernel is compiled for (4, 8, 16)
+  int maxe_t;     // energy slots per home cell the home-cell kernel is compiled for (2, 4, 8, 16)
   int cell_warps; // warps covering the cells of one point (32 x cpl cells per warp)
   int cpl;        // home cells per lane (1..3)
   int ldS;        // floats between the slice rows in shared memory (odd: conflict-free column reads)

@@ -203,7 +203,7 @@ struct Server {
   // Copies one finished batch's results into the callers' buffers (no lock held).
   static std::vector<std::pair<uint64_t, Done>> copy_out(const InFlight& f) {
     std::vector<std::pair<uint64_t, Done>> out(f.reqs.size());
-    const bool overflow = f.ctrl[2] || f.ctrl[5] || f.ctrl[8] || f.ctrl[11];
+    const bool overflow = f.ctrl[2] || f.ctrl[5] || f.ctrl[8] || f.ctrl[11] || f.ctrl[14];
     for (size_t i = 0; i < f.reqs.size(); ++i) {
       const Request& r = f.reqs[i];
       Done& d = out[i].second;
