@@ -554,7 +554,7 @@ def random_walk_requests(n, seed, grids, synth, abi):
     return out
 
 
-SERVE_RATES = tuple((r, 600) for r in (100.0, 250.0, 500.0, 750.0, 1000.0, 1500.0, 2000.0, 3000.0))
+SERVE_RATES = tuple((r, 600) for r in (100.0, 250.0, 500.0, 750.0, 1000.0, 1500.0, 2000.0, 3000.0, 4000.0, 6000.0))
 SERVE_P99_BOUND_MS = 50.0  # the latency bound the sustainable rate is stated against
 
 
