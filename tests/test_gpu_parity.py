@@ -353,11 +353,11 @@ def test_ring_windows_sum_to_full_profile(monkeypatch):
 
 def test_home_cell_kernel_shapes(eng_v171019):
     """Energy grids that select every home-cell kernel shape: at most 2 (the
-    two-slot variant, its own kernel group), up to 8 and up to 16 energies per
-    NSX cell (fewer cells per lane), and a grid spanning two warps of cells
-    (0.02-60 keV), each against the oracle."""
+    two-slot variant, its own kernel group; also over two warps of cells), up
+    to 8 and up to 16 energies per NSX cell (fewer cells per lane), and a grid
+    spanning two warps of cells (0.02-60 keV), each against the oracle."""
     ora = eng_v171019.ora
-    for E in (synth.energy_grid(128, 0.2, 12.0), synth.energy_grid(600, 0.2, 12.0),
+    for E in (synth.energy_grid(128, 0.2, 12.0), synth.energy_grid(160, 0.02, 60.0), synth.energy_grid(600, 0.2, 12.0),
               synth.energy_grid(1100, 0.2, 12.0), synth.energy_grid(400, 0.02, 60.0)):
         g = eng_v171019.add_energy_grid(E)
         p = synth.config2_params(g, -1, n_side=24, n_bins=16)

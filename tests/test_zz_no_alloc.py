@@ -8,7 +8,8 @@ working state in a fixed device array and writes only into buffers the caller
 already owns.  This test (its own file, collected last) allocates the output
 buffers itself and calls the entry point through the C ABI twice in a row
 with different profiles, for each of
-  * the NSX FP32 integrand with the FP64 fold and with the BF16x3 tensor-core fold,
+  * the NSX FP32 integrand with the FP64 fold and with the BF16x3 tensor-core fold
+    (300 energies, and 128 energies: the two-slot home-cell kernel),
   * the blackbody integrand in FP32 and in FP64 (flux only),
 and checks each result against ppm_profile (flux within 1e-12 relative, floor
 1e-6 of the max: the same tiles and partial sums, added to the flux in another
@@ -49,8 +50,12 @@ def setup():
     r = e.add_response(g, rsp)
     E_bb = synth.energy_grid(64, 0.2, 10.0)
     g_bb = e.add_energy_grid(E_bb)
+    E128 = synth.energy_grid(128, 0.2, 12.0)
+    g128 = e.add_energy_grid(E128)
+    rsp128 = synth.response(300, 1000, E128, seed=0)
+    r128 = e.add_response(g128, rsp128)
     env = {"torch": torch, "e": e, "g": g, "r": r, "E": E, "rsp": rsp, "E_bb": E_bb, "g_bb": g_bb,
-           "ora": oracle.Oracle(lens, nsx)}
+           "E128": E128, "g128": g128, "r128": r128, "rsp128": rsp128, "ora": oracle.Oracle(lens, nsx)}
     yield env
     e.close()
 
@@ -69,10 +74,10 @@ def run_noalloc(torch, e, p, n_e, n_ch, flux_d, counts_d):
     return flux, counts, info
 
 
-def nsx_cases(env):
-    first = synth.config2_params(env["g"], env["r"], n_side=48, n_bins=16)
-    second, _ = synth.draw_prior(1, seed=11, lens_u=(0.3, 0.5), n_side=40, n_bins=24, energy_grid=env["g"],
-                                 response=env["r"])
+def nsx_cases(env, grid="g", resp="r"):
+    first = synth.config2_params(env[grid], env[resp], n_side=48, n_bins=16)
+    second, _ = synth.draw_prior(1, seed=11, lens_u=(0.3, 0.5), n_side=40, n_bins=24, energy_grid=env[grid],
+                                 response=env[resp])
     return [first, second[0]]
 
 
@@ -87,7 +92,8 @@ def bb_cases(env, precision):
 
 
 CASES = [("nsx_fold_fp64", _abi.FOLD_FP64), ("nsx_fold_bf16x3", _abi.FOLD_BF16X3),
-         ("blackbody_fp32", _abi.PREC_FP32), ("blackbody_fp64", _abi.PREC_FP64)]
+         ("nsx128_fold_bf16x3", _abi.FOLD_BF16X3), ("blackbody_fp32", _abi.PREC_FP32),
+         ("blackbody_fp64", _abi.PREC_FP64)]
 
 
 @pytest.mark.parametrize("case,mode", CASES, ids=[c[0] for c in CASES])
@@ -96,10 +102,12 @@ def test_noalloc_matches_plain_and_oracle_two_calls(setup, case, mode):
     torch, e = env["torch"], env["e"]
     nsx = case.startswith("nsx")
     if nsx:
-        plist = nsx_cases(env)
+        e128 = case.startswith("nsx128")  # at most two energies per NSX cell: the two-slot kernel
+        plist = nsx_cases(env, "g128", "r128") if e128 else nsx_cases(env)
         for p in plist:
             p.fold = mode
-        E, n_ch, tol = env["E"], 300, TOL32
+        E, n_ch, tol = (env["E128"] if e128 else env["E"]), 300, TOL32
+        rsp = env["rsp128"] if e128 else env["rsp"]
     else:
         plist = bb_cases(env, mode)
         E, n_ch, tol = env["E_bb"], 0, (TOL64 if mode == _abi.PREC_FP64 else TOL32)
@@ -129,7 +137,7 @@ def test_noalloc_matches_plain_and_oracle_two_calls(setup, case, mode):
         assert info.n_clamped == info_ref.n_clamped, case
         if nsx:
             assert max_rel(counts, counts_ref) < tol, case
-            assert max_rel(counts, oracle.fold(env["rsp"], ora_flux, p.exposure_s)) < tol, case
+            assert max_rel(counts, oracle.fold(rsp, ora_flux, p.exposure_s)) < tol, case
     torch.cuda.synchronize()
     assert torch.cuda.mem_get_info()[0] == free_before, "ppm_profile_noalloc changed the device's free memory"
 
