@@ -252,6 +252,7 @@ __device__ __forceinline__ bool in_spot(const DevSpot& s, double c2, double s2, 
 // Per-ring oblate geometry (cpu/devarshi24st_cpu.cpp:90-124).
 struct RingGeom {
   double cos_t, sin_t, R, u, uu, dS, cos_tau, sin_tau, logg;
+  double beta, gamma, dt2;  // the sweep's ring terms: surface speed / c, Lorentz factor, surface-to-R_eq delay
   int i_u;
   double a_u;
   bool u_clamped;
@@ -270,6 +271,15 @@ __device__ inline void ring_geometry(const DevProfile& p, const DevLens& L, doub
   g.dS = g.R * g.R * dOmega * ff;
   g.cos_tau = 1. / ff;
   g.sin_tau = f / ff;
+  // the terms of every fine-phase sample that depend on the ring only (cpu/devarshi24st_cpu.cpp:153-154,
+  // :162-170), computed once here with the sweep's own expressions
+  {
+    const double two_pi = 2. * 3.14159265358979323846;
+    const double c_in_km_s = 299792458. / 1e3;
+    g.beta = two_pi * p.nu * g.R * g.sin_t / g.uu / c_in_km_s;
+    g.gamma = 1. / sqrt(1. - g.beta * g.beta);
+    g.dt2 = (p.Re - g.R + p.Rs * log1p((p.Re - g.R) / (g.R - p.Rs))) / c_in_km_s;
+  }
   double uc = g.u;
   g.u_clamped = (uc < L.u_min) || (uc > L.u_max);
   g.i_u = uhunt(uc, L.u_min, L.u_max, L.n_u, g.a_u);
@@ -322,8 +332,7 @@ __device__ inline bool sweep_sample(const DevProfile& p, const DevLens& L, const
   double cos_sigma = cos_alpha * g.cos_tau +
                      saosp * g.sin_tau * (p.cos_obs * g.sin_t - p.sin_obs * g.cos_t * cos_spot_phi);
   if (cos_sigma <= 0) return false;
-  double beta = two_pi * p.nu * g.R * g.sin_t / g.uu / c_in_km_s;
-  double gamma = 1. / sqrt(1. - beta * beta);
+  const double beta = g.beta, gamma = g.gamma;
   double cos_xi = -saosp * p.sin_obs * sin_spot_phi;
   double delta = 1. / (gamma * (1. - beta * cos_xi));
   double delta3 = delta * delta * delta;
@@ -334,7 +343,7 @@ __device__ inline bool sweep_sample(const DevProfile& p, const DevLens& L, const
                       a_u * a_ca * rows.cdt1[i_ca + 1];
   double dt1 = cdt_over_R * g.R / c_in_km_s;
   double Re = p.Re, Rs = p.Rs;
-  double dt2 = (Re - g.R + Rs * log1p((Re - g.R) / (g.R - Rs))) / c_in_km_s;
+  double dt2 = g.dt2;
   if (!(cos_alpha >= 0)) {
     double tmp = (2. * sin_alpha) / sqrt(3. * (1. - g.u));
     double p_over_R = -tmp * cos((acos(3. * g.u / tmp) + 2. * 3.14159265358979323846) / 3.);
