@@ -779,6 +779,26 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
     G.grid = (int)std::min<long long>((long long)sm_count * occ, std::max(1ll, cap[v]));
     B.groups.push_back(G);
   }
+  // fused point-source mode: one blackbody group, every spot a point source taking the phase-major walk,
+  // at most two flux additions per (bin, energy), so that plain additions give the compensated sum's bits
+  B.fused_points = B.groups.size() == 1 && (vof[0] == 1 || vof[0] == 2);
+  for (int i = 0; i < n && B.fused_points; ++i) {
+    const ppm_params& q = ps[i];
+    bool points = q.n_spots >= 1;
+    for (int k = 0; k < q.n_spots; ++k) points &= q.spots[k].kind == PPM_SPOT_POINT;
+    B.fused_points = points && (long long)grids[q.energy_grid].E.size() <= 4 && q.n_spots * std::max(1, q.n_gl) <= 2;
+  }
+  if (B.fused_points) {
+    BatchImpl::Group& G = B.groups[0];
+    G.args.n_fused = n;
+    G.args.comp = nullptr;
+    G.grid = n;
+    // the queue control words are never written by a fused pass: zero once, for the collect's overflow check
+    if (copy_stream)
+      PPM_CUDA(cudaMemsetAsync(B.d_ctrl, 0, sizeof(int) * 16, copy_stream));
+    else
+      PPM_CUDA(cudaMemset(B.d_ctrl, 0, sizeof(int) * 16));
+  }
   // folds grouped by (response, n_bins, arithmetic)
   std::map<std::tuple<int, int, int>, std::vector<FoldJob>> folds;
   for (int i = 0; i < n; ++i) {
@@ -810,7 +830,7 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
 void Engine::batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events) {
   const int n = B.n;
   if (events) PPM_CUDA(cudaEventRecord(events[0], st));
-  {
+  if (!B.fused_points) {
     NvtxRange range("clear + plan");
     PPM_CUDA(cudaMemsetAsync(B.d_flux, 0, 2 * sizeof(double) * (size_t)std::max(1ll, B.flux_off[n]), st));
     PPM_CUDA(cudaMemsetAsync(B.d_stats, 0, B.small_bytes, st));
@@ -821,8 +841,8 @@ void Engine::batch_enqueue(BatchImpl& B, cudaStream_t st, cudaEvent_t* events) {
   {
     NvtxRange range("integrand");
     for (const auto& G : B.groups) PPM_CUDA(launch_integrand(G.args, G.grid, st));
-    // the compensation pool's rounding errors back into the flux pool
-    PPM_CUDA(launch_add_comp(B.d_flux, B.d_comp, B.flux_off[n], sm_count, st));
+    // the compensation pool's rounding errors back into the flux pool (a fused pass adds plainly)
+    if (!B.fused_points) PPM_CUDA(launch_add_comp(B.d_flux, B.d_comp, B.flux_off[n], sm_count, st));
   }
   if (events) PPM_CUDA(cudaEventRecord(events[2], st));
   NvtxRange fold_range("fold");
@@ -849,6 +869,7 @@ void Engine::batch_launch_timed(BatchImpl& B, cudaStream_t st, float* ms) {
 }
 
 int Engine::kernels_per_pass(const BatchImpl& B) const {
+  if (B.fused_points) return 1 + (int)B.folds.size();          // the fused integrand, folds
   return 2 * (int)B.groups.size() + 1 + (int)B.folds.size();  // plan + integrand per group, add_comp, folds
 }
 

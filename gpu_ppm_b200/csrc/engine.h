@@ -160,6 +160,10 @@ struct BatchImpl {
   cudaGraphExec_t graph = nullptr;
   cudaStream_t last_stream = nullptr;
   int chunk = 1024;                // candidate elements per tile of the home-cell NSX group
+  // one blackbody group whose spots are all point sources, at most two flux additions per (bin, energy): one
+  // fused launch per pass (the integrand plans, clears and integrates each profile; no memsets, no planner,
+  // no compensation pool)
+  bool fused_points = false;
   long long* d_fit_off = nullptr;  // counts offset per profile (fit statistics)
   ppm_fit* d_fit = nullptr;
   BatchImpl() = default;

@@ -128,16 +128,19 @@ __device__ int tile_prologue(const KernelArgs& a, const DevProfile& p, const Dev
   }
   __syncthreads();
   if (n_act == 0) return 0;
+  // counted by the tiles of the first node range only; a ring counts once, by the first of its tiles to
+  // find active elements.  In the fused point-source mode no planner has dropped the ring yet: the counting
+  // waits for the sweep's drop test below
+  auto count_ring = [&]() {
+    atomicAdd(&p.stats[0], (unsigned long long)n_act);
+    const unsigned bit = 1u << (tile.ring & 31);
+    if (!(atomicOr(&p.ring_seen[tile.spot * p.ring_words + (tile.ring >> 5)], bit) & bit))
+      atomicAdd(&p.stats[1], 1ull);
+    if (s_g.u_clamped && tile.first) atomicAdd(&p.stats[4], 1ull);
+  };
+  const bool fused = a.n_fused > 0;
   if (tid == 0) {
-    // counted by the tiles of the first node range only; a ring counts once, by the first of its tiles to
-    // find active elements
-    if (tile.u0 == 0) {
-      atomicAdd(&p.stats[0], (unsigned long long)n_act);
-      const unsigned bit = 1u << (tile.ring & 31);
-      if (!(atomicOr(&p.ring_seen[tile.spot * p.ring_words + (tile.ring >> 5)], bit) & bit))
-        atomicAdd(&p.stats[1], 1ull);
-      if (s_g.u_clamped && tile.first) atomicAdd(&p.stats[4], 1ull);
-    }
+    if (tile.u0 == 0 && !fused) count_ring();
     s_int[40] = p.n_fine + 1;  // invisible min
     s_int[41] = -1;            // invisible max
   }
@@ -175,7 +178,17 @@ __device__ int tile_prologue(const KernelArgs& a, const DevProfile& p, const Dev
   }
   __syncthreads();
   const int inv_min = s_int[40], inv_max = s_int[41];
-  if (inv_min == 0 || inv_max == nf - 1) return 0;  // cpu/devarshi24st_cpu.cpp:195
+  const bool dropped = inv_min == 0 || inv_max == nf - 1;  // cpu/devarshi24st_cpu.cpp:195
+  if (fused && tid == 0) {
+    if (!dropped) {
+      count_ring();
+    } else {  // the planner's count of a dropped ring (plan_kernel)
+      atomicAdd(&p.stats[1], 1ull);
+      atomicAdd(&p.stats[2], 1ull);
+      atomicAdd(&p.stats[5], (unsigned long long)n_act);
+    }
+  }
+  if (dropped) return 0;
   if (inv_min <= inv_max) {
     const int beg = inv_min - 1, end = inv_max + 1;
     const double p0 = s.P[beg], p1 = s.P[end], z0 = s.Z[beg], z1 = s.Z[end];
@@ -1102,6 +1115,14 @@ __device__ __forceinline__ unsigned pm_walk(const SmemPtrs& s, const double* inv
   return n_vis;
 }
 
+// Fused point-source mode: the first point spot k >= k0 of the profile inside the batch's ring window, or
+// n_spots (the tile's own sweep then makes plan_kernel's ring-drop test, tile_prologue).
+__device__ __forceinline__ int fused_next_spot(const DevProfile& pf, int k0) {
+  int k = k0;
+  while (k < pf.n_spots && pf.spot[k].i_lo > pf.spot[k].i_hi) ++k;
+  return k;
+}
+
 template <typename Real, int NE_T>
 __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a) {
   extern __shared__ __align__(16) unsigned char sm[];
@@ -1115,13 +1136,37 @@ __global__ void __launch_bounds__(512, 2) integrand_bb_kernel(const KernelArgs a
   double* b_z = b_c + nt;
   int* b_bin = (int*)(b_z + nt);
 
+  // fused point-source mode: this CTA's profile starts from zero flux and counters (ordered before the tiles'
+  // atomics by the barrier at the top of the loop); each point spot is planned here as the planner would
+  if (a.n_fused > 0) {
+    if ((int)blockIdx.x >= a.n_fused) return;
+    const DevProfile& pf = a.profiles[blockIdx.x];
+    const long long n_flux = (long long)pf.n_bins * pf.n_e;
+    for (long long k = tid; k < n_flux; k += nt) a.flux[pf.flux_off + k] = 0.0;
+    for (int k = tid; k < kStats; k += nt) pf.stats[k] = 0ull;
+    for (int k = tid; k < kMaxSpots * pf.ring_words; k += nt) pf.ring_seen[k] = 0u;
+    if (tid == 0) s_tile = -1;  // the spot last taken
+  }
+  __shared__ Tile s_tile_rec;  // the tile taken (fused mode: built here)
   for (;;) {
     __syncthreads();
-    if (tid == 0) s_tile = atomicAdd(a.queue.next, 1);
+    if (tid == 0) {
+      if (a.n_fused > 0) {
+        const DevProfile& pf = a.profiles[blockIdx.x];
+        const int k = fused_next_spot(pf, s_tile + 1);
+        s_tile = k;
+        s_int[47] = k < pf.n_spots ? 1 : 0;
+        s_tile_rec = Tile{(int)blockIdx.x, (short)k, 1, 0, 0, 1, 0, (short)(pf.n_bins * max(pf.n_gl, 1))};
+      } else {
+        const int t = atomicAdd(a.queue.next, 1);
+        const bool live = t < *a.queue.n_tiles && t < a.queue.capacity;
+        s_int[47] = live ? 1 : 0;
+        if (live) s_tile_rec = a.queue.tiles[t];
+      }
+    }
     __syncthreads();
-    const int t = s_tile;
-    if (t >= *a.queue.n_tiles || t >= a.queue.capacity) break;
-    const Tile tile = a.queue.tiles[t];
+    if (!s_int[47]) break;
+    const Tile tile = s_tile_rec;
     const DevProfile& p = a.profiles[tile.profile];
     const DevSpot& sp = p.spot[tile.spot];
     const bool point = sp.kind == 1;

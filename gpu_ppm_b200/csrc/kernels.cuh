@@ -42,6 +42,9 @@ struct KernelArgs {
   double* flux;  // pool
   double* comp;  // compensation pool of the flux pool's atomic additions (nullptr: plain additions)
   IntegrandShape shape;
+  // > 0: fused point-source mode of the blackbody kernel (no queue, no planner): CTA b takes profile b of
+  // n_fused, clears its flux and counters, drops or integrates each point spot's single tile
+  int n_fused;
 };
 
 // chunk: candidate elements per tile; nodes_per_tile: phase nodes per tile (<= 0: all of a profile's)

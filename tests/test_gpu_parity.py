@@ -4,6 +4,8 @@ reference's own golden vectors.
 Tolerances (tests/errors.py metric, floor 1e-6 of the max):
   * FP32 NSX integrand: 1e-4 relative per bin and per channel;
   * FP64 blackbody integrand: 1e-6 relative."""
+import math
+
 import numpy as np
 import pytest
 
@@ -130,6 +132,45 @@ def test_blackbody_pointwise_and_energy_paths(golden, eng_v200804, ora_v200804):
     fb, _, _ = e.profile_batch([many, p1], want_flux=True, want_counts=False)
     assert max_rel(fb[0], ref_many) < TOL64
     assert max_rel(fb[1], few[1][1]) < TOL64
+    e.close()
+
+
+def test_fused_point_source_pass():
+    """A batch whose spots are all point sources (one or two energies here,
+    at most two flux additions per bin and energy) runs as one fused launch:
+    each CTA clears, plans and integrates its profile.  It gives the bits and
+    the counters of the planned pass (the same profile batched with a
+    HEALPix spot), and matches the oracle; a point source hidden at phase 0
+    is dropped and counted as the planner counts it."""
+    lens = synth.lensing("std")
+    e = Engine()
+    e.load_lensing(lens)
+    ora = oracle.Oracle(lens)
+    E1, E2 = np.array([1.0]), np.array([0.8, 2.0])
+    g1, g2 = e.add_energy_grid(E1), e.add_energy_grid(E2)
+    cases = []
+    for prec, tol in ((_abi.PREC_FP32, TOL32), (_abi.PREC_FP64, TOL64)):
+        for g, E, n_gl, th, inc in ((g1, E1, 0, 90.0, 90.0), (g2, E2, 2, 60.0, 30.0), (g1, E1, 0, 178.0, 5.0)):
+            p = synth.params(mass_msun=1.4, r_eq_km=12.0, spin_hz=600.0, inclination_rad=inc * math.pi / 180,
+                             distance_kpc=0.2, spots=[synth.spot(th * math.pi / 180, 0.0, 0.01, kT_keV=0.35,
+                                                                 kind=_abi.SPOT_POINT)],
+                             atmosphere=_abi.ATM_BLACKBODY, n_side=64, n_bins=64, n_gl=n_gl, energy_grid=g,
+                             precision=prec)
+            cases.append((p, E, tol, th))
+    for p, E, tol, th in cases:
+        f_fused, _, info = e.profile(p, want_counts=False)
+        q = synth.config1_params(p.energy_grid)
+        q.precision = p.precision
+        fb, _, infos = e.profile_batch([q, p], want_flux=True, want_counts=False)
+        assert np.array_equal(np.asarray(f_fused).reshape(-1), np.asarray(fb[1]).reshape(-1)), th
+        for k in ("n_active", "n_rings", "n_dropped_rings", "n_points", "n_clamped", "n_active_integrated"):
+            assert getattr(info, k) == getattr(infos[1], k), (th, k)
+        ref, oinfo = ora.profile(p, E)
+        assert info.n_points == oinfo.n_points and info.n_dropped_rings == oinfo.n_dropped_rings, th
+        if th > 170:
+            assert info.n_dropped_rings == 1 and not np.asarray(f_fused).any()
+        else:
+            assert info.n_dropped_rings == 0 and max_rel(f_fused, ref) < tol, th
     e.close()
 
 
