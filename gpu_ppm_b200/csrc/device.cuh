@@ -13,6 +13,8 @@
 namespace ppm {
 
 constexpr int kMaxSpots = 2;
+// doubles per fine phase k in DevProfile::fine: cos(2 pi k / n_fine), sin(2 pi k / n_fine), k / n_fine
+constexpr int kFineStride = 3;
 // per-profile counters: active (integrated rings), rings, dropped rings, points, clamped, active (dropped rings)
 constexpr int kStats = 6;
 
@@ -77,7 +79,7 @@ struct DevProfile {
   int n_side, n_bins, n_gl, n_fine, n_spots, atmosphere, interp, beaming, precision, n_e;
   long long flux_off;   // doubles into the flux pool
   const double* ring;   // [4 n_side] (z, cos(acos z), sin(acos z)) per ring index i (entry 0 unused)
-  const double* fine;   // [n_fine] (cos 2 pi k/n, sin 2 pi k/n)
+  const double* fine;   // [n_fine][kFineStride] (cos 2 pi k/n, sin 2 pi k/n, k/n)
   DevGrid grid;
   unsigned long long* stats;  // [kStats]
   unsigned* ring_seen;        // [kMaxSpots][ring_words] bits: rings already counted in stats[1]
@@ -313,9 +315,9 @@ __device__ inline bool sweep_sample(const DevProfile& p, const DevLens& L, const
                                     int i_phase, bool nsx, double& F, double& Z, double& P, double& MU) {
   const double two_pi = 2. * 3.14159265358979323846;
   const double c_in_km_s = 299792458. / 1e3;
-  double phase = 1. * i_phase / p.n_fine;
-  double cos_spot_phi = p.fine[2 * i_phase];
-  double sin_spot_phi = p.fine[2 * i_phase + 1];
+  double phase = p.fine[kFineStride * i_phase + 2];  // 1. * i_phase / n_fine, divided on the host
+  double cos_spot_phi = p.fine[kFineStride * i_phase];
+  double sin_spot_phi = p.fine[kFineStride * i_phase + 1];
   double cos_psi = p.cos_obs * g.cos_t + p.sin_obs * g.sin_t * cos_spot_phi;
   if (cos_psi < L.cp_min) return false;
   double sin_psi = sqrt(1. - cos_psi * cos_psi);

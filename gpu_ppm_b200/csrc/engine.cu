@@ -423,12 +423,13 @@ void compute_ring_rows(int N, std::vector<double>& h) {
 }
 
 void compute_fine_rows(int nf, std::vector<double>& h) {
-  h.resize(2 * (size_t)nf);
+  h.resize(kFineStride * (size_t)nf);
   for (int k = 0; k < nf; ++k) {
     double phase = 1. * k / nf;
     double spot_phi = two_pi * phase;
-    h[2 * k] = std::cos(spot_phi);
-    h[2 * k + 1] = std::sin(spot_phi);
+    h[kFineStride * k] = std::cos(spot_phi);
+    h[kFineStride * k + 1] = std::sin(spot_phi);
+    h[kFineStride * k + 2] = phase;  // the sweep's phase, the same IEEE division as on the device
   }
 }
 
@@ -443,7 +444,7 @@ const double* Engine::ring_table(int N) {
   return d;
 }
 
-// (cos, sin) of 2 pi k / n_fine (cpu/devarshi24st_cpu.cpp:131-134).
+// (cos, sin) of 2 pi k / n_fine and k / n_fine (cpu/devarshi24st_cpu.cpp:131-134).
 const double* Engine::fine_table(int nf) {
   auto it = fine_tabs.find(nf);
   if (it != fine_tabs.end()) return it->second;

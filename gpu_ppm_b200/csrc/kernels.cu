@@ -2,7 +2,9 @@
 // FP64/FP32 variants) and SIMT response folds.
 //
 // Integrand structure (one CTA per tile = candidate elements of one ring of
-// one spot of one profile; CTAs pull tiles from a device queue):
+// one spot of one profile; CTAs pull tiles from a device queue, except in the
+// blackbody kernel's fused point-source mode, where CTA b takes profile b's
+// point spots without a planner):
 //   1. ring geometry                      cpu/devarshi24st_cpu.cpp:90-124
 //   2. active-element compaction by warp ballot + prefix (deterministic order)
 //                                         gpu/devarshi24st_gpu.cu:196-212

@@ -117,7 +117,7 @@ void Engine::profile_noalloc(const ppm_params& p, double* flux_d, double* counts
   const size_t o_ring = off;
   off += up256(sizeof(double) * 3 * 4 * (size_t)N);
   const size_t o_fine = off;
-  off += up256(sizeof(double) * 2 * (size_t)nf);
+  off += up256(sizeof(double) * kFineStride * (size_t)nf);
   GridSplit split;
   if (nsx_atm) split_grid(gr.E, nsx.inv_dE, split);
   const size_t n_cf = nsx_atm ? split.cell_first.size() : 1;
