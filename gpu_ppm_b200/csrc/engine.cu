@@ -795,10 +795,12 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
     G.args.comp = nullptr;
     G.grid = n;
     // the queue control words are never written by a fused pass: zero once, for the collect's overflow check
+    // (a synchronous copy when there is no copy stream, complete before the batch is launched on any stream)
+    const int zeros[16] = {0};
     if (copy_stream)
-      PPM_CUDA(cudaMemsetAsync(B.d_ctrl, 0, sizeof(int) * 16, copy_stream));
+      PPM_CUDA(cudaMemcpyAsync(B.d_ctrl, zeros, sizeof(zeros), cudaMemcpyHostToDevice, copy_stream));
     else
-      PPM_CUDA(cudaMemset(B.d_ctrl, 0, sizeof(int) * 16));
+      PPM_CUDA(cudaMemcpy(B.d_ctrl, zeros, sizeof(zeros), cudaMemcpyHostToDevice));
   }
   // folds grouped by (response, n_bins, arithmetic)
   std::map<std::tuple<int, int, int>, std::vector<FoldJob>> folds;
