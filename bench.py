@@ -567,7 +567,7 @@ def sustainable(curve, bound_ms=SERVE_P99_BOUND_MS):
 
 def serving_bench(lens, nsx, synth, abi, Engine, device, rates=SERVE_RATES):
     """Open-loop Poisson request streams through ppm_submit (continuous batching), one per offered rate."""
-    eng = Engine(device=device, n_streams=2)
+    eng = Engine(device=device, n_streams=3)
     eng.load_lensing(lens)
     eng.load_nsx(nsx)
     grids = {}

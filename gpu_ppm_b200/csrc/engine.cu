@@ -149,7 +149,7 @@ void HostBuffer::release() {
 
 Engine::Engine(const ppm_engine_config& c) : cfg(c) {
   if (cfg.memory_budget <= 0) cfg.memory_budget = 64ll << 30;
-  if (cfg.n_streams <= 0) cfg.n_streams = 2;
+  if (cfg.n_streams <= 0) cfg.n_streams = 3;
   if (cfg.max_batch <= 0) cfg.max_batch = 1 << 16;
   block_cache.set_limit((size_t)cfg.memory_budget);
   int n_dev = 0;

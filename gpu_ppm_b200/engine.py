@@ -19,7 +19,7 @@ from ._abi import check, dptr, lib
 
 
 class Engine:
-    def __init__(self, device=0, max_batch=65536, memory_budget=0, autotune=0, n_streams=2):
+    def __init__(self, device=0, max_batch=65536, memory_budget=0, autotune=0, n_streams=3):
         cfg = _abi.EngineConfig(device, max_batch, memory_budget, autotune, n_streams)
         h = ctypes.c_void_p()
         check(lib().ppm_engine_create(ctypes.byref(cfg), ctypes.byref(h)))

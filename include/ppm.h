@@ -165,9 +165,9 @@ typedef struct ppm_engine_config {
   int64_t memory_budget;      /* bytes of device memory for in-flight request state (0 = 64 GiB); also
                                  the most device memory the engine keeps cached between synchronous calls */
   int32_t autotune;           /* 1: time candidate launch shapes at first use */
-  int32_t n_streams;          /* serving: concurrent batches in flight (0 = 2: one computing while the next
-                                 is staged); the server also pins n_streams + 4 staging buffers of 32 MiB
-                                 when it starts (first ppm_submit) */
+  int32_t n_streams;          /* serving: concurrent batches in flight (0 = 3: batches overlap on the GPU
+                                 while the next is staged); the server also pins n_streams + 4 staging
+                                 buffers of 32 MiB when it starts (first ppm_submit) */
 } ppm_engine_config;
 
 /* ---- engine ---------------------------------------------------------------- */
