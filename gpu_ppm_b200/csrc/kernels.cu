@@ -78,6 +78,7 @@ struct SmemPtrs {
   unsigned char* batch;
   float4* Q;
   float* H;
+  unsigned short* hidx;  // home-cell kernel: bracket table of phase_o (see node_point_tab)
 };
 
 __device__ __forceinline__ SmemPtrs carve(unsigned char* sm, const IntegrandShape& S) {
@@ -93,6 +94,7 @@ __device__ __forceinline__ SmemPtrs carve(unsigned char* sm, const IntegrandShap
   s.batch = sm + S.off_batch;
   s.Q = (float4*)(sm + S.off_Q);
   s.H = (float*)(sm + S.off_Q + (S.nsx ? S.pb * S.cells * 16 : 0));
+  s.hidx = (unsigned short*)(sm + S.off_hidx);
   return s;
 }
 
@@ -240,6 +242,34 @@ __device__ __forceinline__ double node_point(const DevProfile& p, const SmemPtrs
   if (patch < s.P[0]) patch += 1.;
   double af;
   const int i = vhunt(s.P, p.n_fine + 1, patch, af);
+  const double flux = (1 - af) * s.F[i] + af * s.F[i + 1];
+  if (flux == 0) return 0.0;
+  z = (1 - af) * s.Z[i] + af * s.Z[i + 1];
+  mu = (1 - af) * s.MU[i] + af * s.MU[i + 1];
+  return flux;
+}
+
+// node_point with the tile's bracket table hidx (hidx[k] = vhunt's bracket of
+// phase_o[0] + k / n_fine): on a non-decreasing phase_o (mono) the bracket of
+// the patch phase is walked to from its table entry, a step or none, and is
+// vhunt's bracket exactly; the fraction and the lerps are node_point's.
+__device__ __forceinline__ double node_point_tab(const DevProfile& p, const SmemPtrs& s, const RingPhi& rp, bool point,
+                                                 int jj, double ppt, bool mono, double& z, double& mu) {
+  const double phi = point ? 0.0 : rp.dphi * (s.j[jj] - rp.jofs);
+  const double phase_shift = phi / kTwoPi;
+  const double xph = ppt + phase_shift + 1.;
+  double patch = xph - floor(xph);
+  if (patch < s.P[0]) patch += 1.;
+  const int n = p.n_fine + 1;
+  double af;
+  int i;
+  if (mono) {
+    const int k = clampi((int)((patch - s.P[0]) * p.n_fine), 0, p.n_fine);
+    i = walk_bracket(s.P, n, patch, s.hidx[k]);
+    af = (patch - s.P[i]) / (s.P[i + 1] - s.P[i]);
+  } else {
+    i = vhunt(s.P, n, patch, af);
+  }
   const double flux = (1 - af) * s.F[i] + af * s.F[i + 1];
   if (flux == 0) return 0.0;
   z = (1 - af) * s.Z[i] + af * s.Z[i + 1];
@@ -779,7 +809,17 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
     }
     for (int k = tid; k < nmu; k += nt) s.mu[k] = X.mu[k];
     for (int k = tid; k < 4 * (nmu - 3); k += nt) s.mu[nmu + k] = X.mu_den[k];
-    __syncthreads();
+    // the tile's phase_o bracket table for node_point_tab, used where phase_o is non-decreasing
+    bool mono_ok = true;
+    {
+      const int n_fp = p.n_fine + 1;
+      for (int k = tid; k < p.n_fine; k += nt) mono_ok &= s.P[k + 1] >= s.P[k];
+      for (int k = tid; k <= p.n_fine; k += nt) {
+        double a_unused;
+        s.hidx[k] = (unsigned short)vhunt(s.P, n_fp, s.P[0] + (double)k / p.n_fine, a_unused);
+      }
+    }
+    const bool mono = __syncthreads_and(mono_ok) != 0;
     // slice rows 0..nE-1 start 16-byte aligned after room for rows -2, -1; rows nE, nE + 1 follow them
     float* const Sx = s.S + ((2 * ldS + 3) & ~3);
     {
@@ -886,7 +926,7 @@ __global__ void __launch_bounds__(NTMAX, MINB) integrand_nsx_cell_kernel(const K
         const int jj = jb + st;
         if (jj < n_act) {
           double z = 0, mu = 0;
-          const double flux = node_point(p, s, rp, point, jj, s_ppt[set], z, mu);
+          const double flux = node_point_tab(p, s, rp, point, jj, s_ppt[set], mono, z, mu);
           if (flux != 0.0) {
             vis = true;
             if (mu < s.mu[nmu - 1]) mu = s.mu[nmu - 1];
@@ -1644,6 +1684,8 @@ IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int 
     s.off_batch = off;
     s.off_Q = off;
     off += al((long)nt * 32);
+    s.off_hidx = off;
+    off += al((long)nf1 * 2);
     s.total = off;
     return s;
   }

@@ -29,6 +29,7 @@ struct IntegrandShape {
   int ldS;        // floats between the slice rows in shared memory (odd: conflict-free column reads)
   // offsets in bytes
   int off_j, off_P, off_F, off_Z, off_MU, off_mu, off_S, off_union, off_rows, off_batch, off_Q, total;
+  int off_hidx;   // home-cell kernel: the tile's phase_o bracket table ([n_fine + 1] uint16), 0 elsewhere
 };
 
 IntegrandShape make_shape(bool nsx, int nt, int ne_t, int pb, int max_cand, int n_fine, int n_cp, int n_ca, int nE,
