@@ -565,6 +565,22 @@ def sustainable(curve, bound_ms=SERVE_P99_BOUND_MS):
     return max(ok, key=lambda r: r["offered_req_per_s"]) if ok else None
 
 
+def trace_summary(trace, after_us):
+    """Per-rate batch figures from ppm_serve_trace: the batches admitted after after_us, their request counts,
+    the host time from admission to the last enqueue (build + enqueue), the device time from the enqueue to
+    the finish callback, and the publish time (results copied into the callers' buffers)."""
+    bs = [b for b in trace if b["t_admit"] > after_us]
+    if not bs:
+        return {"batches": 0}
+    build = [(b["t_launched"] - b["t_admit"]) / 1000.0 for b in bs]
+    gpu = [(b["t_finished"] - b["t_launched"]) / 1000.0 for b in bs]
+    pub = [(b["t_published"] - b["t_finished"]) / 1000.0 for b in bs]
+    nreq = [b["n_requests"] for b in bs]
+    return {"batches": len(bs), "batch_requests_max": int(max(nreq)), "batch_requests_mean": float(np.mean(nreq)),
+            "build_ms_max": float(max(build)), "gpu_ms_p50": float(np.percentile(gpu, 50)),
+            "gpu_ms_max": float(max(gpu)), "publish_ms_max": float(max(pub))}
+
+
 def serving_bench(lens, nsx, synth, abi, Engine, device, rates=SERVE_RATES):
     """Open-loop Poisson request streams through ppm_submit (continuous batching), one per offered rate."""
     eng = Engine(device=device, n_streams=3)
@@ -584,6 +600,7 @@ def serving_bench(lens, nsx, synth, abi, Engine, device, rates=SERVE_RATES):
     for t in [eng.submit(p, None, b) for p, b in zip(warm, bufs)]:
         eng.wait(t)
         eng.release(t)
+    t_seen = max([-1.0] + [b["t_admit"] for b in eng.serve_trace()])  # batches before this admit time are done
     # one request stream for every offered rate (the same sampler walk, so the rates see the same request mix)
     stream_reqs = random_walk_requests(max(n for _, n in rates), 1000, grids, synth, abi)
     for k, (rate, n) in enumerate(rates):
@@ -608,10 +625,13 @@ def serving_bench(lens, nsx, synth, abi, Engine, device, rates=SERVE_RATES):
             lat.append(eng.latency_us(t) / 1000.0)
             eng.release(t)
         t_all = time.perf_counter() - t0
-        results.append({"offered_req_per_s": rate, "requests": n, "throughput_req_per_s": n / t_all,
-                        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                        "max_ms": float(np.max(lat)), "client_lag_ms_max": float(np.max(lag)),
-                        "submit_ms_p50": float(np.percentile(sub, 50)), "submit_ms_max": float(np.max(sub))})
+        row = {"offered_req_per_s": rate, "requests": n, "throughput_req_per_s": n / t_all,
+               "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+               "max_ms": float(np.max(lat)), "client_lag_ms_max": float(np.max(lag)),
+               "submit_ms_p50": float(np.percentile(sub, 50)), "submit_ms_max": float(np.max(sub))}
+        row.update(trace_summary(eng.serve_trace(), t_seen))
+        t_seen = max([t_seen] + [b["t_admit"] for b in eng.serve_trace()])
+        results.append(row)
     eng.close()
     return results
 

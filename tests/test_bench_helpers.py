@@ -60,3 +60,16 @@ def test_sustainable_rate_is_the_highest_rate_kept_up_with_under_the_bound():
     assert bench.sustainable(curve, 50.0)["offered_req_per_s"] == 1000  # 1500 is not kept up with
     assert bench.sustainable(curve, 10.0)["offered_req_per_s"] == 100
     assert bench.sustainable(curve, 1.0) is None
+
+
+def test_trace_summary_counts_only_the_batches_admitted_after_the_mark():
+    def batch(admit, launched, finished, published, n):
+        return {"t_admit": admit, "t_launched": launched, "t_finished": finished, "t_published": published,
+                "n_requests": n, "stream_slot": 0, "staging_bytes": 0}
+
+    trace = [batch(10, 20, 1020, 1030, 4), batch(2000, 2500, 4500, 4510, 8), batch(3000, 3100, 9100, 9300, 2)]
+    s = bench.trace_summary(trace, 10)
+    assert s["batches"] == 2 and s["batch_requests_max"] == 8 and s["batch_requests_mean"] == 5.0
+    assert s["build_ms_max"] == 0.5 and s["gpu_ms_max"] == 6.0 and s["gpu_ms_p50"] == 4.0
+    assert s["publish_ms_max"] == 0.2
+    assert bench.trace_summary(trace, 5000) == {"batches": 0}
