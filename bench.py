@@ -600,7 +600,10 @@ def serving_bench(lens, nsx, synth, abi, Engine, device, rates=SERVE_RATES):
     for t in [eng.submit(p, None, b) for p, b in zip(warm, bufs)]:
         eng.wait(t)
         eng.release(t)
-    t_seen = max([-1.0] + [b["t_admit"] for b in eng.serve_trace()])  # batches before this admit time are done
+    try:  # batches admitted up to this time belong to the warm-up
+        t_seen = max([-1.0] + [b["t_admit"] for b in eng.serve_trace()])
+    except Exception:  # noqa: BLE001
+        t_seen = -1.0
     # one request stream for every offered rate (the same sampler walk, so the rates see the same request mix)
     stream_reqs = random_walk_requests(max(n for _, n in rates), 1000, grids, synth, abi)
     for k, (rate, n) in enumerate(rates):
@@ -629,8 +632,12 @@ def serving_bench(lens, nsx, synth, abi, Engine, device, rates=SERVE_RATES):
                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                "max_ms": float(np.max(lat)), "client_lag_ms_max": float(np.max(lag)),
                "submit_ms_p50": float(np.percentile(sub, 50)), "submit_ms_max": float(np.max(sub))}
-        row.update(trace_summary(eng.serve_trace(), t_seen))
-        t_seen = max([t_seen] + [b["t_admit"] for b in eng.serve_trace()])
+        try:  # diagnostics only: never lose the curve to them
+            trace = eng.serve_trace()
+            row.update(trace_summary(trace, t_seen))
+            t_seen = max([t_seen] + [b["t_admit"] for b in trace])
+        except Exception as exc:  # noqa: BLE001
+            row["trace_error"] = repr(exc)
         results.append(row)
     eng.close()
     return results

@@ -732,10 +732,22 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
   B.d_comp = B.d_flux + std::max(1ll, B.flux_off[n]);
   B.d_counts = (double*)B.mem.alloc(sizeof(double) * (size_t)std::max(1ll, B.counts_off[n]));
   Tile* tiles = (Tile*)B.mem.alloc(sizeof(Tile) * (size_t)std::max(1ll, cap_total));
-  if (copy_stream)  // pageable source: returns once staged, ordered on the batch's stream
-    PPM_CUDA(cudaMemcpyAsync(B.d_prof, hp.data(), sizeof(DevProfile) * (size_t)n, cudaMemcpyHostToDevice, copy_stream));
-  else
-    PPM_CUDA(cudaMemcpy(B.d_prof, hp.data(), sizeof(DevProfile) * (size_t)n, cudaMemcpyHostToDevice));
+  // uploads: from the caller's pinned area when it has room (asynchronous), else from the pageable source (the
+  // copy returns once the source is staged, ordered on the batch's stream), else synchronous
+  size_t staged = 0;
+  auto upload = [&](void* dst, const void* src, size_t bytes) {
+    if (copy_stream && B.h_upload && staged + bytes <= B.h_upload_cap) {
+      unsigned char* h = (unsigned char*)B.h_upload + staged;
+      std::memcpy(h, src, bytes);
+      staged += (bytes + 255) & ~(size_t)255;
+      PPM_CUDA(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, copy_stream));
+    } else if (copy_stream) {
+      PPM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, copy_stream));
+    } else {
+      PPM_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    }
+  };
+  upload(B.d_prof, hp.data(), sizeof(DevProfile) * (size_t)n);
   B.h2d_bytes = sizeof(DevProfile) * (size_t)n;
   long long base = 0;
   B.groups.clear();
@@ -797,10 +809,7 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
     // the queue control words are never written by a fused pass: zero once, for the collect's overflow check
     // (a synchronous copy when there is no copy stream, complete before the batch is launched on any stream)
     const int zeros[16] = {0};
-    if (copy_stream)
-      PPM_CUDA(cudaMemcpyAsync(B.d_ctrl, zeros, sizeof(zeros), cudaMemcpyHostToDevice, copy_stream));
-    else
-      PPM_CUDA(cudaMemcpy(B.d_ctrl, zeros, sizeof(zeros), cudaMemcpyHostToDevice));
+    upload(B.d_ctrl, zeros, sizeof(zeros));
   }
   // folds grouped by (response, n_bins, arithmetic)
   std::map<std::tuple<int, int, int>, std::vector<FoldJob>> folds;
@@ -819,11 +828,7 @@ void Engine::batch_build(BatchImpl& B, int n, const ppm_params* ps, cudaStream_t
   }
   if (!jobs.empty()) {
     B.d_jobs = (FoldJob*)B.mem.alloc(sizeof(FoldJob) * jobs.size());
-    if (copy_stream)
-      PPM_CUDA(cudaMemcpyAsync(B.d_jobs, jobs.data(), sizeof(FoldJob) * jobs.size(), cudaMemcpyHostToDevice,
-                               copy_stream));
-    else
-      PPM_CUDA(cudaMemcpy(B.d_jobs, jobs.data(), sizeof(FoldJob) * jobs.size(), cudaMemcpyHostToDevice));
+    upload(B.d_jobs, jobs.data(), sizeof(FoldJob) * jobs.size());
     B.h2d_bytes += sizeof(FoldJob) * jobs.size();
   }
 }

@@ -157,6 +157,10 @@ struct BatchImpl {
   std::vector<Group> groups;
   std::vector<Fold> folds;
   size_t h2d_bytes = 0;
+  // pinned host memory the build stages its uploads in, when given (serving: one area per stream slot, untouched
+  // until the slot's batch has finished, so the copies run asynchronously); pageable copies otherwise
+  void* h_upload = nullptr;
+  size_t h_upload_cap = 0;
   cudaGraphExec_t graph = nullptr;
   cudaStream_t last_stream = nullptr;
   int chunk = 1024;                // candidate elements per tile of the home-cell NSX group

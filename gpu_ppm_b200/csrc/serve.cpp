@@ -52,6 +52,8 @@ HostBuffer take(HostBuffer& b) {
 // bytes it stages, and only a single request larger than a buffer gets its own.
 constexpr size_t kStageBytes = size_t(32) << 20;
 constexpr size_t kStageFixed = 64 + 256;  // control words and slack around the per-request arrays
+// a full batch's uploads (profiles, fold jobs, control words), each rounded up to 256 bytes
+constexpr size_t kUploadBytes = kMaxRequestsPerBatch * (sizeof(DevProfile) + sizeof(FoldJob)) + 4 * 256;
 
 size_t staged_bytes(size_t n, size_t counts, size_t flux, bool want_flux) {
   return kStageFixed + sizeof(unsigned long long) * kStats * n + sizeof(double) * (counts + (want_flux ? flux : 0));
@@ -76,6 +78,7 @@ struct Server {
   struct Slot {
     cudaStream_t stream = nullptr;
     bool busy = false;
+    HostBuffer upload;  // pinned source of the batch build's uploads; reused once the slot's batch has finished
   };
   struct InFlight {
     std::vector<Request> reqs;
@@ -129,10 +132,13 @@ struct Server {
       // in flight, kMaxCompleting - 1 queued and one being copied out
       stage_pool.resize(slots.size() + kMaxCompleting);
       for (auto& b : stage_pool) b.reserve(kStageBytes);
+      for (auto& s : slots) s.upload.reserve(kUploadBytes);
     } catch (...) {  // the destructor does not run for a constructor that throws
       for (auto& b : stage_pool) b.release();
-      for (auto& s : slots)
+      for (auto& s : slots) {
         if (s.stream) cudaStreamDestroy(s.stream);
+        s.upload.release();
+      }
       throw;
     }
     // keep freed stream-ordered memory in the pool instead of returning it each time
@@ -163,6 +169,7 @@ struct Server {
         cudaStreamSynchronize(s.stream);
         cudaStreamDestroy(s.stream);
       }
+      s.upload.release();
     }
     for (auto& b : stage_pool) b.release();
   }
@@ -346,6 +353,8 @@ struct Server {
     f.B.reset(new BatchImpl());
     BatchImpl& B = *f.B;
     B.mem.stream = slot.stream;
+    B.h_upload = slot.upload.ptr;
+    B.h_upload_cap = slot.upload.cap;
     {
       std::lock_guard<std::mutex> elk(eng->mu);
       eng->batch_build(B, n, ps.data(), slot.stream);
