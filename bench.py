@@ -485,7 +485,7 @@ def main():
                 "visible_points_per_launch": points, "evaluations_per_launch": evals,
                 "note": "the convention counts 80 FLOP per evaluation; the kernel contracts mu once per slice row "
                         "and builds each cubic once per cell per phase point, so it executes fewer operations per "
-                        "evaluation and frac can exceed 1; its hardware bound is instruction issue with the FMA and ALU pipes (74 % of issue "
+                        "evaluation and frac can exceed 1; its hardware bound is instruction issue with the FMA and ALU pipes (76 % of issue "
                         "slots in the ncu capture of a 96-profile launch)",
             },
             "phases_ms": {"clear_plan": float(ph[0]), "integrand": float(ph[1]), "fold": float(ph[2])},
