@@ -167,7 +167,8 @@ typedef struct ppm_engine_config {
   int32_t autotune;           /* 1: time candidate launch shapes at first use */
   int32_t n_streams;          /* serving: concurrent batches in flight (0 = 3: batches overlap on the GPU
                                  while the next is staged); the server also pins n_streams + 4 staging
-                                 buffers of 32 MiB when it starts (first ppm_submit) */
+                                 buffers of 32 MiB and, per stream, a small upload area for the batch
+                                 build's host-to-device copies when it starts (first ppm_submit) */
 } ppm_engine_config;
 
 /* ---- engine ---------------------------------------------------------------- */
